@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the Indigo2 SSSP/BFS/CC relaxation path on B200.
+
+Workload (one GPU): SSSP on an RMAT graph of scale 22 (4,194,304 vertices,
+edge factor 16, a=0.57 b=0.19 c=0.19 d=0.05, seed 22), symmetrised,
+deduplicated, no self-loops, int32 weights uniform in [1,255] (one per
+undirected edge), source = highest-degree vertex (lowest ID on ties); fixed
+style: edge-centric data-driven push (the engine's vp_cta: one thread per
+frontier edge). A step is one complete SSSP traversal (init + all iterations)
+with the graph resident in HBM; nlist + eweight (1 GB) exceed L2, so every step
+streams them from HBM.
+
+value   : GTEPS, reference definition (1e-9 * g.edges / seconds per traversal,
+          include/bfs_vertex_cuda.h:163), summed over all ranks.
+e2e     : the same metric through the public C ABI from pinned host buffers:
+          i2_graph_upload (H2D of nindex/nlist/eweight) + i2_sssp (D2H of dist)
+          + i2_graph_free, per step.
+roofline: the relax kernel, from algorithmic bytes B_alg = 12*E_r + 20*V_r
+          (E_r = sum of degrees of reached vertices, V_r = reached vertices)
+          over the sum of its launch durations (CUDA events on its stream).
+Multi-GPU (torchrun): independent replicas, one per rank ("replicas only":
+a single traversal does not shard); timing is the max over ranks.
+
+--impl reference: the reference's own CPU SSSP (codes/cpp/sssp-cpp
+V_Data_Push ... NonDup, its fastest CPU SSSP; built unchanged into oracle/_ref)
+on the same graph with all host threads, one traversal per step, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GTEPS & HBM GB/s: learned-style vs best fixed style, BFS/SSSP/CC bit-exact"
+UNIT = "GTEPS"
+WORKLOAD = {"workload": "sssp_rmat22_ef16_edge_data_push", "graph": "rmat", "scale": 22, "edge_factor": 16,
+            "a": 0.57, "b": 0.19, "c": 0.19, "seed": 22, "weights": "uniform[1,255]",
+            "source": "highest-degree vertex", "algorithm": "sssp", "style": "vp_cta (edge-centric data-driven push)",
+            "l2": "inputs larger than L2 (nlist+eweight 1.0 GB)"}
+SELECTOR_PARAMS = ROOT / "indigo2suite_b200" / "selector_params.bin"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    def __init__(self, world: int, backend: str):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as td
+
+            td.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.td = td
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, x: float, device) -> float:
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+_PINNED = []
+
+
+def pinned_copy(a: np.ndarray) -> np.ndarray:
+    import torch
+
+    t = torch.empty(a.size, dtype=torch.int32, pin_memory=True)
+    _PINNED.append(t)  # keeps the page-locked buffer alive for the numpy view
+    out = t.numpy()
+    out[:] = a
+    return out
+
+
+def graph_source(g) -> int:
+    return int(np.argmax(g.degrees()))  # first maximum: lowest ID on ties
+
+
+def ref_cpu_baseline(g, src: int, runs: int, name: str) -> dict:
+    import oracle
+
+    threads = os.cpu_count() or 1
+    ts = []
+    for _ in range(runs):
+        t, _ = oracle.ref_cpu_run(name, g, src, threads)
+        ts.append(t)
+    med = statistics.median(ts)
+    return {"value": 1e-9 * g.edges / med, "unit": UNIT, "cores": threads, "kind": "reference",
+            "program": name, "sample": f"full workload graph, {runs} traversals, median of the reference's own timer"}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    import oracle
+
+    import indigo2suite_b200 as i2  # host generator only (same CSR as the device generator)
+
+    if not (oracle.REF_OUT / "libref_cpu_sssp_vertex_cpp.so").exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference CPU programs)"}))
+        return
+    g = i2.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
+    src = graph_source(g)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.ref_cpu_run("sssp_vertex_cpp", g, src, threads)
+    ts = []
+    for _ in range(args.steps):
+        t, _ = oracle.ref_cpu_run("sssp_vertex_cpp", g, src, threads)
+        ts.append(t)
+    total = sum(ts)
+    value = 1e-9 * g.edges * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": dict(WORKLOAD, reference_program="sssp_vertex_cpp"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": "full workload graph, one traversal per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local: int):
+    import torch
+
+    import indigo2suite_b200 as i2
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    dg = i2.DeviceGraph.generate_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
+    host = dg.download()
+    E, V = host.edges, host.nodes
+    src = graph_source(host)
+    variant = args.variant
+
+    # correctness of the measured configuration (shortest-path certificate)
+    d, rep = dg.sssp(src, variant=variant)
+    import oracle
+
+    cert = oracle.certify_distances(host, src, d, weighted=True)
+    if cert is not None:
+        raise SystemExit(f"result certificate failed: {cert}")
+
+    def steps(n, v=variant):
+        for _ in range(n):
+            dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, report=False)
+
+    with torch.cuda.stream(stream):
+        steps(args.warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    steps(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_max = dist.max(ms, dev)
+    value = world * 1e-9 * E / (ms_max * 1e-3)
+
+    # dominant kernel: relax launches timed one by one with CUDA events (host-driven loop)
+    rep_h = dg.run_device(i2.I2_SSSP, src, variant=variant, loop=i2.I2_LOOP_HOST, stream=sp)
+    rep_g = dg.run_device(i2.I2_SSSP, src, variant=variant, stream=sp)
+    b_alg = 12.0 * rep_g.reached_edges + 20.0 * rep_g.reached_vertices
+    achieved = b_alg / rep_h.relax_seconds / 1e9
+    peak, peak_kind = peaks()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": peak_kind,
+                "kernel": f"relax_push<SSSP,{variant}>", "launches_per_step": rep_g.iterations,
+                "b_alg_bytes_per_step": b_alg, "relax_ms_per_step_events": 1e3 * rep_h.relax_seconds,
+                "relax_ms_per_step_device_timer": 1e3 * rep_g.relax_seconds}
+    prof = ROOT / "profiles" / "relax_sssp_rmat22_traffic.json"
+    if prof.exists():
+        tr = json.loads(prof.read_text())
+        roofline["traffic"] = tr.get("dram_bytes_per_step")
+        roofline["traffic_note"] = tr.get("note")
+
+    # the other styles and the selectors (a few steps each)
+    styles = {}
+    cand = list(range(i2.I2_NUM_VARIANTS)) + ["heuristic"]
+    if SELECTOR_PARAMS.exists():
+        i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
+        cand.append("learned")
+    for v in cand:
+        name = v if isinstance(v, str) else i2.VARIANTS[v]
+        if v in (4, 5) and not dg.info["symmetric"]:
+            continue
+        with torch.cuda.stream(stream):
+            steps(1, v)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        steps(args.style_steps, v)
+        f1.record(stream)
+        f1.synchronize()
+        styles[name] = 1e-9 * E / (f0.elapsed_time(f1) / args.style_steps * 1e-3)
+    fixed = {k: v for k, v in styles.items() if k not in ("heuristic", "learned")}
+
+    # end to end through the C ABI from pinned host buffers
+    hp = i2.ECLGraph(V, E, pinned_copy(host.nindex), pinned_copy(host.nlist), pinned_copy(host.eweight))
+    out = pinned_copy(np.zeros(V, np.int32))
+    ts = []
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gg = i2.DeviceGraph.upload(hp)
+        gg.sssp(src, variant=variant, out=out)
+        gg.free()
+        torch.cuda.synchronize()
+        if k > 0:
+            ts.append(time.perf_counter() - t0)
+    e2e_s = dist.max(statistics.median(ts), dev)
+    e2e = {"value": world * 1e-9 * E / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 4 * (V + 1) + 8 * E, "d2h_bytes_per_step": 4 * V,
+           "ms_per_step": 1e3 * e2e_s,
+           "query_only_note": "per-query C-ABI call on a resident graph: see e2e_query"}
+    q0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        dg.sssp(src, variant=variant, out=out)
+    q_s = (time.perf_counter() - q0) / args.e2e_steps
+    e2e_query = {"value": world * 1e-9 * E / dist.max(q_s, dev), "unit": UNIT, "h2d_bytes_per_step": 4,
+                 "d2h_bytes_per_step": 4 * V}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = ref_cpu_baseline(host, src, 3, "sssp_vertex_cpp")
+            g18 = i2.gen_rmat(18, 16, 0.57, 0.19, 0.19, seed=22)
+            same = ref_cpu_baseline(g18, graph_source(g18), 1, "sssp_edge_cpp")
+            cpu["same_style"] = {"program": "sssp_edge_cpp (E_Data_Push)", "value": same["value"],
+                                 "sample": "RMAT scale 18 (same parameters), 1 traversal"}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    launches = args.steps * (3 + rep_g.iterations)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_query": e2e_query,
+            "gpu_launches": launches, "clocks": clk,
+            "styles_gteps": styles, "best_fixed_style": max(fixed, key=fixed.get),
+            "iterations": rep_g.iterations, "reached_vertices": rep_g.reached_vertices,
+            "reached_edges": rep_g.reached_edges, "verified": "shortest-path certificate"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dg.free()
+    dist.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--variant", default="vp_cta")
+    ap.add_argument("--style-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if world != args.gpus and not (world == 1 and args.gpus == 1):
+        if rank == 0:
+            print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

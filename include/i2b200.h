@@ -1,0 +1,215 @@
+/*
+ * i2b200 — B200 (sm_100a) engine for the edge-relaxation hot path of the
+ * Indigo2 suite: BFS levels, SSSP distances and connected-component labels on
+ * ECLgraph CSR graphs. Plain C ABI: host pointers, sizes and status codes.
+ *
+ * Reference interfaces replaced (paths inside the Indigo2Suite project):
+ *   struct ECLgraph, readECLgraph, writeECLgraph, freeECLgraph  include/ECLgraph.h:44-106
+ *   static double GPUbfs_vertex(int src, const ECLgraph&, int* dist)    include/bfs_vertex_cuda.h:61
+ *   static double GPUbfs_edge(int src, const ECLgraph&, int* dist, const int* sp)  include/bfs_edge_cuda.h:61
+ *   static double GPUsssp_vertex(...)  include/sssp_vertex_cuda.h:60
+ *   static double GPUsssp_edge(...)    include/sssp_edge_cuda.h:60
+ *   static double GPUcc_vertex(const ECLgraph&, int* label)              include/cc_vertex_cuda.h:57
+ *   static double GPUcc_edge(const ECLgraph&, int* label, const int* sp) include/cc_edge_cuda.h:57
+ *   synthetic SSSP weights 1 + (i*nei) % nodes                          include/sssp_vertex_cuda.h:127-137
+ *   starting-point array sp[]                                           include/bfs_edge_cuda.h:140-146
+ * Unlike the reference, no function here calls exit(): every failure is a
+ * status code (the reference exits in CheckCuda(), include/bfs_vertex_cuda.h:101-109).
+ */
+#ifndef I2B200_H
+#define I2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  I2_OK = 0,
+  I2_ERR_ARG = 1,         /* null pointer, source out of range, bad size or option */
+  I2_ERR_IO = 2,          /* file could not be opened, read or written */
+  I2_ERR_FORMAT = 3,      /* malformed or truncated ECLgraph file or CSR */
+  I2_ERR_NOMEM = 4,       /* host or device allocation failed */
+  I2_ERR_CUDA = 5,        /* CUDA runtime error */
+  I2_ERR_NO_DEVICE = 6,   /* no CUDA device */
+  I2_ERR_UNSUPPORTED = 7, /* variant not applicable to this graph (pull on a directed graph) */
+  I2_ERR_ITER_CAP = 8,    /* iteration cap reached before the fixed point */
+  I2_ERR_OVERFLOW = 9     /* int32 limit or capacity exceeded */
+} i2_status;
+
+/* Host CSR graph. Layout-identical to struct ECLgraph (include/ECLgraph.h:44-50). */
+typedef struct {
+  int nodes;
+  int edges;
+  int* nindex;  /* nodes + 1 */
+  int* nlist;   /* edges */
+  int* eweight; /* edges, or NULL */
+} i2_eclgraph;
+
+/* Algorithms. */
+enum { I2_BFS = 0, I2_SSSP = 1, I2_CC = 2 };
+
+/* Relaxation variants (styles). Every variant reaches the same fixed point. */
+enum {
+  I2_AUTO_HEURISTIC = -1, /* per-iteration choice by a fixed frontier-size rule */
+  I2_AUTO_LEARNED = -2,   /* per-iteration choice by the on-device MLP selector */
+  I2_VP_THREAD = 0,       /* vertex push, data-driven, thread per frontier vertex */
+  I2_VP_WARP = 1,         /* vertex push, data-driven, warp per frontier vertex */
+  I2_VP_CTA = 2,          /* edge-balanced push: thread per frontier edge */
+  I2_VP_BLOCK = 3,        /* vertex push, data-driven, block per frontier vertex */
+  I2_PULL_FRONTIER = 4,   /* pull from frontier neighbours (bottom-up); symmetric graphs */
+  I2_PULL_TOPO = 5,       /* topology-driven pull from all neighbours; symmetric graphs */
+  I2_EDGE_TOPO = 6,       /* edge-centric sweep over all CSR entries */
+  I2_PUSH_TOPO = 7,       /* topology sweep of the frontier bitmap, thread per vertex */
+  I2_NUM_VARIANTS = 8
+};
+
+/* Loop modes. */
+enum {
+  I2_LOOP_GRAPH = 0, /* whole traversal is one CUDA graph with a device-side while loop */
+  I2_LOOP_HOST = 1   /* host launches each iteration and reads the frontier size back */
+};
+
+typedef struct {
+  int variant;      /* I2_VP_* ... or I2_AUTO_* */
+  int loop_mode;    /* I2_LOOP_GRAPH (default 0) or I2_LOOP_HOST */
+  int iter_cap;     /* 0: default cap of nodes + 2 launches (enough for every algorithm) */
+  int record_iters; /* 1: keep per-iteration records (i2_get_records) */
+  void* stream;     /* cudaStream_t to run on; NULL: the graph's own stream */
+} i2_opts;
+
+typedef struct {
+  double seconds;          /* device time of init + all iterations (CUDA events) */
+  double relax_seconds;    /* sum of the relax launches' device durations */
+  int iterations;          /* relax launches */
+  int variant_hist[16];    /* launches per variant */
+  long long reached_vertices;
+  long long reached_edges; /* sum of degrees of reached vertices */
+} i2_report;
+
+/* Per-iteration record (one per relax launch). */
+typedef struct {
+  int iter;
+  int variant;
+  int size;                /* light frontier entries consumed */
+  int hsize;               /* heavy frontier entries consumed */
+  unsigned long long edges;/* frontier edges consumed */
+  int maxdeg;
+  int mindist;
+  long long visited;       /* vertices reached before this launch */
+  unsigned long long t_ns; /* launch duration (device timer) */
+  float feat[16];          /* selector features of the consumed frontier */
+} i2_iter_record;
+
+typedef struct {
+  int nodes;
+  int edges;
+  int maxdeg;
+  int nheavy;
+  int wmin;
+  int symmetric;
+  int has_weights;
+  float avgdeg;
+  float degcv;
+} i2_graph_info;
+
+typedef struct i2_graph i2_graph;
+
+/* ---- library ---- */
+const char* i2_status_string(int status);
+const char* i2_variant_name(int variant);
+int i2_version(void);
+int i2_device_count(void);
+
+/* ---- ECLgraph files (include/ECLgraph.h:52-106; errors are status codes) ---- */
+int i2_read_eclgraph(const char* path, i2_eclgraph* out);
+int i2_write_eclgraph(const i2_eclgraph* g, const char* path);
+void i2_free_eclgraph(i2_eclgraph* g);
+/* Allocate an empty graph of the given size (nindex zeroed; eweight if weighted). */
+int i2_alloc_eclgraph(int nodes, int edges, int weighted, i2_eclgraph* out);
+/* Fill eweight with the reference's synthetic weights (include/sssp_vertex_cuda.h:127-137). */
+int i2_synth_weights(i2_eclgraph* g);
+/* Host starting-point array sp[e] = source vertex of CSR entry e (include/bfs_edge_cuda.h:140-146). */
+int i2_build_sp(const i2_eclgraph* g, int* sp);
+
+/* ---- seeded synthetic graphs (host, OpenMP). Symmetrised, deduplicated, no
+   self-loops, sorted adjacency; weights uniform in [1,255], one per undirected edge. ---- */
+int i2_gen_er(int n, long long m, uint64_t seed, int weighted, i2_eclgraph* out);
+int i2_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                int weighted, i2_eclgraph* out);
+/* RMAT on n vertices (n need not be a power of two): scale ceil(log2 n),
+   edge_factor * 2^scale samples, endpoints >= n rejected after relabelling. */
+int i2_gen_rmat_n(int n, int edge_factor, double a, double b, double c, uint64_t seed, int weighted,
+                  i2_eclgraph* out);
+int i2_gen_grid(int side, double remove_frac, double add_frac, uint64_t seed, int weighted,
+                i2_eclgraph* out);
+
+/* ---- device graphs ---- */
+/* Copy a host CSR to the device and compute its statistics. */
+int i2_graph_upload(const i2_eclgraph* host, i2_graph** out);
+/* Wrap CSR arrays already on the device (the reference harness's d_g, include/bfs_vertex_cuda.h:140-144).
+   The arrays stay owned by the caller and must outlive the handle. */
+int i2_graph_wrap_device(const i2_eclgraph* dev, i2_graph** out);
+/* Generate an RMAT graph directly on the device (identical CSR to i2_gen_rmat). */
+int i2_graph_generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                           int weighted, i2_graph** out);
+int i2_graph_info_get(const i2_graph* g, i2_graph_info* out);
+/* Copy the device CSR back to a host graph allocated by the callee. */
+int i2_graph_download(const i2_graph* g, i2_eclgraph* out);
+/* Launch tuning of a graph: degree threshold from which a frontier vertex is
+   split across the whole grid (heavy path), and resident blocks per SM of the
+   relax kernels. 0 keeps the current value. Results do not depend on either. */
+int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm);
+/* Give the graph the reference's synthetic weights when it has none (on the device). */
+int i2_graph_synth_weights(i2_graph* g);
+int i2_graph_free(i2_graph* g);
+
+/* ---- traversals (replace GPU<alg>_<vertex|edge>) ----
+   dist/label are HOST arrays of g.nodes ints, filled before return. */
+int i2_bfs(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep);
+int i2_sssp(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep);
+int i2_cc(i2_graph* g, int* label, const i2_opts* opts, i2_report* rep);
+/* Same, with the result left in (or copied to) DEVICE memory; out_dev may be NULL
+   to keep the result only inside the engine. src is ignored for I2_CC. */
+int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* opts, i2_report* rep);
+/* Records of the last traversal run with record_iters = 1. */
+int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n);
+
+/* Per-iteration sweep for selector training: follows the trajectory of `follow`
+   and times every allowed variant from each iteration's state (state saved and
+   restored on the device). times[it * I2_NUM_VARIANTS + v] in ns (-1: not allowed). */
+int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_record* recs,
+             float* times, int cap, int* n);
+
+/* ---- learned selector ---- */
+/* Number of floats in the MLP parameter blob (normaliser + 16-64-64-8 weights). */
+int i2_mlp_param_count(void);
+/* Install the selector's parameters on the current device. */
+int i2_mlp_set_params(const float* params, int count);
+/* One forward + backward pass of the masked-MSE loss on the device (hand-written
+   kernels). X: n x 16 features, T: n x 8 targets, M: n x 8 mask. Outputs the loss
+   and the gradient w.r.t. every parameter (same layout as the blob). */
+int i2_mlp_loss_grad(const float* params, const float* X, const float* T, const float* M, int n,
+                     float* loss, float* grad);
+/* Train on the device with Adam for `epochs` passes of minibatches of `batch` rows;
+   params is read as the initial point and overwritten with the result. */
+int i2_mlp_train(float* params, const float* X, const float* T, const float* M, int n, int epochs,
+                 int batch, float lr, uint64_t seed, float* final_loss);
+/* Device inference on n feature rows; writes the chosen variant per row (mask of allowed variants). */
+int i2_mlp_predict(const float* params, const float* X, int n, int allowed_mask, int* choice);
+
+/* ---- batches of graphs traversed together ---- */
+typedef struct i2_batch i2_batch;
+int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out);
+/* dist: host array of sum(nodes) ints, graph k's vertices at offset voff[k]. */
+int i2_batch_run(i2_batch* b, int algo, const int* srcs, int* dist, const i2_opts* opts, i2_report* rep);
+int i2_batch_offsets(const i2_batch* b, long long* voff);
+int i2_batch_free(i2_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* I2B200_H */

@@ -1,0 +1,175 @@
+// Shared device-side definitions of the B200 relaxation engine.
+//
+// The engine computes the same fixed points as the Indigo2 suite's BFS, SSSP and
+// CC codes: BFS levels (codes/cuda/bfs-cuda/*, relax `atomicMin(&dist[dst], s+1)`,
+// e.g. BFS_CUDA_V_Data_Push_..._Warp_..._NonDup.cu:73-79), SSSP distances with
+// int32 weights (SSSP_CUDA_E_Data_Push_..._NonDup.cu:72-73) and CC minimum-ID
+// labels (CC_CUDA_E_Data_Push_..._NonDup.cu:68-71). All values are int32 and
+// INT_MAX marks an unreached vertex, as in include/bfs_vertex_cuda.h:46.
+//
+// Frontier contract shared by every variant (so a selector may switch variant
+// at any iteration without changing the result):
+//   at the start of iteration i, F_i is stored in slot s = i % 3 as
+//     wl[s][0..size)    light vertices (degree < heavy threshold),
+//     hwl[s][0..hsize)  heavy vertices,
+//     bm[s]             a bitmap with exactly the bits of F_i set;
+//   every vertex outside F_i has already relaxed all of its out-edges against
+//   the current dist[]. Iteration i propagates at least F_i and builds F_{i+1}
+//   in slot (i+1) % 3 from every vertex whose value it lowered. It also clears
+//   slot (i+2) % 3 (F_{i-1}), which no variant reads during iteration i.
+#pragma once
+#include <cstdint>
+#include <climits>
+#include <cuda_runtime.h>
+
+namespace i2 {
+
+constexpr int kInf = INT_MAX;
+constexpr int kBlock = 256;          // threads per block for all relax kernels
+constexpr int kWarp = 32;
+constexpr int kQueue = 2048;         // per-block shared staging queue (light)
+constexpr int kHQueue = 128;         // per-block shared staging queue (heavy)
+constexpr int kHeavyTile = 2048;     // edges per tile of a heavy vertex
+constexpr int kMaxVariants = 16;
+constexpr int kFeatures = 16;        // selector input width
+constexpr int kHidden = 64;          // selector hidden width (two layers)
+
+enum Algo { kBFS = 0, kSSSP = 1, kCC = 2 };
+
+enum Variant {
+  kVPThread = 0,     // vertex push, data-driven, thread per frontier vertex
+  kVPWarp = 1,       // vertex push, data-driven, warp per frontier vertex, 128-bit loads
+  kVPCta = 2,        // edge-balanced push: block-scan of a frontier chunk, thread per edge
+  kVPBlock = 3,      // vertex push, data-driven, block per frontier vertex
+  kPullFrontier = 4, // pull from neighbours that are in the frontier bitmap (bottom-up)
+  kPullTopo = 5,     // topology-driven pull over all vertices and all neighbours
+  kEdgeTopo = 6,     // edge-centric sweep over all CSR entries gated by the bitmap
+  kPushTopo = 7,     // topology sweep of the frontier bitmap, thread per vertex
+  kNumVariants = 8
+};
+
+// Device view of a CSR graph in the ECLgraph layout (include/ECLgraph.h:44-50).
+struct DGraph {
+  int nodes;
+  int edges;
+  const int* __restrict__ nindex;   // nodes + 1
+  const int* __restrict__ nlist;    // edges
+  const int* __restrict__ eweight;  // edges (SSSP only)
+  const int* __restrict__ sp;       // edges: source vertex of each CSR entry (edge sweeps only)
+  int vec_ok;                       // 1 when nlist/eweight bases are 16-byte aligned
+};
+
+// Whole-graph statistics used by the selector and the pull bound.
+struct GStats {
+  int nodes;
+  int edges;
+  int maxdeg;
+  int nheavy;       // vertices with degree >= heavy threshold
+  int wmin;         // minimum edge weight (1 for BFS)
+  int symmetric;    // 1 when every (u,v,w) has a (v,u,w) partner
+  float avgdeg;
+  float degcv;      // coefficient of variation of the degree distribution
+};
+
+// Statistics of one frontier buffer, accumulated while it is built.
+struct Slot {
+  int size;                 // light entries
+  int hsize;                // heavy entries
+  unsigned long long edges; // sum of degrees over all entries
+  int maxdeg;
+  int mindist;              // smallest value pushed into this frontier
+  int pad[2];
+};
+
+struct Ctl {
+  Slot slot[3];
+  int iter;                 // index of the next relax launch
+  int iter_cap;
+  int status;               // error bits, see kStatus*
+  int variant;              // variant to run at the next launch
+  unsigned done;            // blocks finished in the current launch
+  int chunk;                // dynamic chunk counter of the current launch
+  unsigned long long tstart;// earliest block start of the current launch (globaltimer ns)
+  long long visited;        // vertices reached so far
+  int hist[kMaxVariants];   // launches per variant
+  int mode;                 // 0 fixed, 1 heuristic, 2 learned
+  int fixed_variant;
+  int allowed;              // bitmask of variants allowed on this graph
+  int src;                  // source vertex (BFS/SSSP)
+  int nsrc;                 // number of sources (batched runs)
+  int algo;
+  int pad[2];
+  unsigned long long relax_ns;  // sum of relax launch durations
+  float feat[kFeatures];    // features of the frontier the next launch consumes
+};
+
+enum : int {
+  kStatusIterCap = 1,
+  kStatusOverflow = 2,
+};
+
+// One record per relax launch: the frontier it consumed and its duration.
+struct IterRec {
+  int iter;
+  int variant;
+  int size;
+  int hsize;
+  unsigned long long edges;
+  int maxdeg;
+  int mindist;
+  long long visited;
+  unsigned long long t_ns;
+  float feat[kFeatures];
+};
+
+// Everything a relax kernel needs, passed by value.
+struct Ctx {
+  DGraph g;
+  GStats gs;
+  int* dist;
+  int* wl[3];
+  int* hwl[3];
+  unsigned* bm[3];
+  Ctl* ctl;
+  IterRec* recs;
+  int rec_cap;
+  int heavy;                // degree threshold of the heavy list
+  int bm_words;             // words per bitmap
+  const float* mlp;         // selector weights (device), may be null
+  const int* srcs;          // batched sources (device), may be null
+  unsigned long long loop_h;   // cudaGraphConditionalHandle of the while node
+  unsigned long long switch_h; // cudaGraphConditionalHandle of the switch node
+  int use_loop;
+  int use_switch;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Relaxation operators: candidate value for dst from source value du along CSR entry k.
+template <int ALG>
+struct Op;
+
+template <>
+struct Op<kBFS> {
+  static __device__ __forceinline__ bool valid(int du) { return du != kInf; }
+  static __device__ __forceinline__ int cand(int du, int /*w*/) { return du + 1; }
+  static constexpr bool kWeighted = false;
+};
+template <>
+struct Op<kSSSP> {
+  static __device__ __forceinline__ bool valid(int du) { return du != kInf; }
+  static __device__ __forceinline__ int cand(int du, int w) { return du + w; }
+  static constexpr bool kWeighted = true;
+};
+template <>
+struct Op<kCC> {
+  static __device__ __forceinline__ bool valid(int) { return true; }
+  static __device__ __forceinline__ int cand(int du, int) { return du; }
+  static constexpr bool kWeighted = false;
+};
+
+}  // namespace i2

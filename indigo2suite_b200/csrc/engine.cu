@@ -1,0 +1,1239 @@
+// B200 relaxation engine: device graphs, traversal runs and the C ABI of
+// include/i2b200.h for BFS, SSSP and CC.
+//
+// A traversal is: reset the control block, fill dist/labels and seed F_0
+// (k_fill, k_seed), then one relax launch per iteration until the frontier is
+// empty (the do-while of the reference's host drivers, e.g.
+// BFS_CUDA_V_Data_Push_..._Warp_..._NonDup.cu:112-122). In the default loop
+// mode the whole sequence is one CUDA graph: a WHILE conditional node whose
+// body is either the fixed variant's relax kernel or a SWITCH node over all
+// variants. The relax kernels' last block decides both conditions on the
+// device, so there is no host round trip per iteration.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+#include "../../include/i2b200.h"
+#include "common.cuh"
+#include "engine.h"
+#include "host_graph.h"
+#include "mlp.cuh"
+#include "relax.cuh"
+
+namespace i2 {
+
+static_assert(sizeof(IterRec) == sizeof(i2_iter_record), "record layout");
+static_assert((int)kNumVariants == (int)I2_NUM_VARIANTS, "variant count");
+
+// ---------------------------------------------------------------------------
+// Selection of the next variant.
+
+__device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, int hsize,
+                              unsigned long long edges) {
+  const float fs = (float)size + (float)hsize;
+  const float fe = (float)edges;
+  const float E = (float)gs.edges;
+  auto ok = [&](int v) { return (allowed >> v) & 1; };
+  if (algo == kBFS && ok(kPullFrontier) && fe > E * (1.f / 16.f)) return kPullFrontier;
+  if (ok(kEdgeTopo) && fe > E * 0.5f) return kEdgeTopo;
+  const float mean = fe / fmaxf(1.f, fs);
+  if (mean >= 64.f && ok(kVPWarp)) return kVPWarp;
+  return ok(kVPCta) ? kVPCta : kVPThread;
+}
+
+// Executed by every thread of one block. Computes the features of the frontier
+// in slot `nxt`, picks the variant for the next launch and sets the graph's
+// switch condition. `cond` tells whether another launch will happen.
+__device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
+  __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], y[kOut];
+  Ctl* ctl = c.ctl;
+  if (threadIdx.x == 0) {
+    volatile Slot* sl = &ctl->slot[nxt];
+    frontier_features(c.gs, ctl->algo, next_iter, sl->size, sl->hsize, sl->edges, sl->maxdeg,
+                      *(volatile long long*)&ctl->visited, x);
+    for (int k = 0; k < kFeatures; ++k) ctl->feat[k] = x[k];
+  }
+  __syncthreads();
+  const int mode = ctl->mode;
+  if (mode == 2 && c.mlp && cond) mlp_forward_block(c.mlp, x, h1, h2, y);
+  if (threadIdx.x == 0) {
+    int v = ctl->fixed_variant;
+    if (mode == 1 || (mode == 2 && !c.mlp)) {
+      volatile Slot* sl = &ctl->slot[nxt];
+      v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, sl->size, sl->hsize, sl->edges);
+    } else if (mode == 2) {
+      float best = 3.0e38f;
+      v = -1;
+      for (int k = 0; k < kOut; ++k)
+        if (((ctl->allowed >> k) & 1) && y[k] < best) {
+          best = y[k];
+          v = k;
+        }
+      if (v < 0) v = kVPThread;
+    }
+    ctl->variant = v;
+    if (cond) ctl->hist[v] += 1;
+    if (c.use_switch) cudaGraphSetConditional((cudaGraphConditionalHandle)c.switch_h, cond ? (unsigned)v : 0xffffu);
+    if (c.use_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)c.loop_h, cond ? 1u : 0u);
+  }
+}
+
+// Last block of a relax launch: record the launch, advance the iteration and
+// decide whether the loop continues.
+__device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old) {
+  __shared__ int s_cond;
+  Ctl* ctl = c.ctl;
+  if (threadIdx.x == 0) {
+    const unsigned long long t1 = globaltimer();
+    const unsigned long long dt = t1 - ctl->tstart;
+    ctl->relax_ns += dt;
+    volatile Slot* sc = &ctl->slot[cur];
+    if (c.recs && i < c.rec_cap) {
+      IterRec& r = c.recs[i];
+      r.iter = i;
+      r.variant = ctl->variant;
+      r.size = sc->size;
+      r.hsize = sc->hsize;
+      r.edges = sc->edges;
+      r.maxdeg = sc->maxdeg;
+      r.mindist = sc->mindist;
+      r.visited = *(volatile long long*)&ctl->visited;
+      r.t_ns = dt;
+      for (int k = 0; k < kFeatures; ++k) r.feat[k] = ctl->feat[k];
+    }
+    Slot& so = ctl->slot[old];
+    so.size = 0;
+    so.hsize = 0;
+    so.edges = 0;
+    so.maxdeg = 0;
+    so.mindist = kInf;
+    ctl->done = 0;
+    ctl->chunk = 0;
+    ctl->tstart = ~0ull;
+    ctl->iter = i + 1;
+    volatile Slot* sn = &ctl->slot[nxt];
+    const long long n = (long long)sn->size + sn->hsize;
+    int cond = n > 0;
+    if (cond && i + 1 >= ctl->iter_cap) {
+      ctl->status |= kStatusIterCap;
+      cond = 0;
+    }
+    s_cond = cond;
+  }
+  __syncthreads();
+  select_next(c, i + 1, nxt, s_cond != 0);
+}
+
+// ---------------------------------------------------------------------------
+// Init kernels.
+
+// dist[v] = INF (BFS/SSSP) or v (CC). For CC every vertex enters F_0.
+template <int ALG>
+__global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
+  __shared__ Stage s;
+  stage_init(s);
+  __syncthreads();
+  const int V = c.g.nodes;
+  for (long long base = (long long)blockIdx.x * kBlock; base < V; base += (long long)gridDim.x * kBlock) {
+    const int v = (int)base + threadIdx.x;
+    const bool in = v < V;
+    if (in) c.dist[v] = (ALG == kCC) ? v : kInf;
+    if (ALG == kCC) {
+      const unsigned word = __ballot_sync(0xffffffffu, in);
+      if ((threadIdx.x & 31) == 0 && word) c.bm[0][v >> 5] = word;
+      if (in) {
+        atomicMin(&s.mindist, v);
+        stage_vertex(c, s, 0, v);
+      }
+      stage_flush(c, s, 0);
+    }
+  }
+  if (ALG == kCC) {
+    stage_flush(c, s, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Slot& sl = c.ctl->slot[0];
+      if (s.edges) atomicAdd(&sl.edges, s.edges);
+      if (s.maxdeg) atomicMax(&sl.maxdeg, s.maxdeg);
+      if (s.mindist != kInf) atomicMin(&sl.mindist, s.mindist);
+    }
+  }
+}
+
+// One block: seed the sources (BFS/SSSP) and select the first variant.
+template <int ALG>
+__global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
+  Ctl* ctl = c.ctl;
+  if (ALG != kCC) {
+    const int ns = c.srcs ? ctl->nsrc : 1;
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+      const int v = c.srcs ? c.srcs[j] : ctl->src;
+      const unsigned bit = 1u << (v & 31);
+      if (atomicOr(&c.bm[0][v >> 5], bit) & bit) continue;
+      c.dist[v] = 0;
+      const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
+      Slot& sl = ctl->slot[0];
+      atomicAdd(&sl.edges, (unsigned long long)deg);
+      atomicMax(&sl.maxdeg, deg);
+      atomicMin(&sl.mindist, 0);
+      atomicAdd((unsigned long long*)&ctl->visited, 1ull);
+      if (deg >= c.heavy) c.hwl[0][atomicAdd(&sl.hsize, 1)] = v;
+      else c.wl[0][atomicAdd(&sl.size, 1)] = v;
+    }
+  } else if (threadIdx.x == 0) {
+    ctl->visited = c.g.nodes;
+  }
+  __threadfence();
+  __syncthreads();
+  select_next(c, 0, 0, true);
+}
+
+// Per-run parameters, passed by value to k_reset so that queued runs never
+// share a host buffer.
+struct RunParams {
+  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap;
+  bool operator!=(const RunParams& o) const { return std::memcmp(this, &o, sizeof(RunParams)) != 0; }
+};
+
+__global__ void k_reset(Ctl* ctl, RunParams p) {
+  if (threadIdx.x != 0) return;
+  unsigned* w = reinterpret_cast<unsigned*>(ctl);
+  for (unsigned k = 0; k < sizeof(Ctl) / sizeof(unsigned); ++k) w[k] = 0u;
+  for (int k = 0; k < 3; ++k) ctl->slot[k].mindist = kInf;
+  ctl->tstart = ~0ull;
+  ctl->iter_cap = p.iter_cap;
+  ctl->mode = p.mode;
+  ctl->fixed_variant = p.fixed_variant;
+  ctl->variant = p.fixed_variant;
+  ctl->allowed = p.allowed;
+  ctl->src = p.src;
+  ctl->nsrc = p.nsrc;
+  ctl->algo = p.algo;
+}
+
+// ---------------------------------------------------------------------------
+// Graph maintenance kernels.
+
+__global__ void k_validate(DGraph g, int* bad) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long v = tid; v < g.nodes; v += stride)
+    if (g.nindex[v + 1] < g.nindex[v]) atomicOr(bad, 1);
+  for (long long e = tid; e < g.edges; e += stride)
+    if ((unsigned)g.nlist[e] >= (unsigned)g.nodes) atomicOr(bad, 2);
+  if (tid == 0 && (g.nindex[0] != 0 || g.nindex[g.nodes] != g.edges)) atomicOr(bad, 4);
+}
+
+struct DevStats {
+  int maxdeg;
+  int nheavy;
+  int wmin;
+  int unsorted;
+  int asym;
+  int pad;
+  double sumsq;
+};
+
+__global__ void k_degree_stats(DGraph g, int heavy, DevStats* st) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int mx = 0, nh = 0, uns = 0;
+  double s2 = 0.0;
+  for (long long v = tid; v < g.nodes; v += stride) {
+    const int b = g.nindex[v], e = g.nindex[v + 1];
+    const int d = e - b;
+    mx = max(mx, d);
+    nh += d >= heavy;
+    s2 += (double)d * d;
+    for (int k = b + 1; k < e && !uns; ++k) uns |= g.nlist[k] <= g.nlist[k - 1];
+  }
+  int wmin = INT_MAX;
+  if (g.eweight)
+    for (long long e = tid; e < g.edges; e += stride) wmin = min(wmin, g.eweight[e]);
+  atomicMax(&st->maxdeg, mx);
+  atomicAdd(&st->nheavy, nh);
+  atomicMin(&st->wmin, wmin);
+  if (uns) atomicOr(&st->unsorted, 1);
+  atomicAdd(&st->sumsq, s2);
+}
+
+// For every entry (u, v, w): is (v, u, w) present? Binary search (adjacency sorted).
+__global__ void k_symmetry(DGraph g, DevStats* st) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int asym = 0;
+  for (long long v = tid; v < g.nodes && !asym; v += stride) {
+    for (int k = g.nindex[v]; k < g.nindex[v + 1]; ++k) {
+      const int u = g.nlist[k];
+      int lo = g.nindex[u], hi = g.nindex[u + 1] - 1, pos = -1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int x = g.nlist[mid];
+        if (x == (int)v) { pos = mid; break; }
+        if (x < (int)v) lo = mid + 1; else hi = mid - 1;
+      }
+      if (pos < 0 || (g.eweight && g.eweight[pos] != g.eweight[k])) { asym = 1; break; }
+    }
+  }
+  if (asym) atomicOr(&st->asym, 1);
+}
+
+__global__ void k_build_sp(DGraph g, int* sp) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long v = tid; v < g.nodes; v += stride)
+    for (int k = g.nindex[v]; k < g.nindex[v + 1]; ++k) sp[k] = (int)v;
+}
+
+// Reference synthetic weights (include/sssp_vertex_cuda.h:127-137) on the device.
+__global__ void k_synth_weights(DGraph g, int* w) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = tid; i < g.nodes; i += stride)
+    for (int j = g.nindex[i]; j < g.nindex[i + 1]; ++j) {
+      const int prod = (int)((unsigned)i * (unsigned)g.nlist[j]);
+      int x = 1 + (prod % g.nodes);
+      w[j] = x < 0 ? -x : x;
+    }
+}
+
+// Reached vertices and the sum of their degrees (E_r).
+__global__ void k_reached(DGraph g, const int* dist, unsigned long long* out) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned long long nv = 0, ne = 0;
+  for (long long v = tid; v < g.nodes; v += stride)
+    if (dist[v] != kInf) {
+      nv++;
+      ne += (unsigned long long)(g.nindex[v + 1] - g.nindex[v]);
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    nv += __shfl_down_sync(0xffffffffu, nv, o);
+    ne += __shfl_down_sync(0xffffffffu, ne, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&out[0], nv);
+    atomicAdd(&out[1], ne);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel tables.
+
+typedef void (*KernelFn)(Ctx);
+
+template <int ALG>
+static KernelFn relax_fn(int v) {
+  switch (v) {
+    case kVPThread: return relax_push<ALG, kVPThread>;
+    case kVPWarp: return relax_push<ALG, kVPWarp>;
+    case kVPCta: return relax_push<ALG, kVPCta>;
+    case kVPBlock: return relax_push<ALG, kVPBlock>;
+    case kPullFrontier: return relax_pull<ALG, true>;
+    case kPullTopo: return relax_pull<ALG, false>;
+    case kEdgeTopo: return relax_edge_topo<ALG>;
+    case kPushTopo: return relax_push_topo<ALG>;
+  }
+  return nullptr;
+}
+
+KernelFn relax_kernel(int algo, int v) {
+  if (algo == kBFS) return relax_fn<kBFS>(v);
+  if (algo == kSSSP) return relax_fn<kSSSP>(v);
+  return relax_fn<kCC>(v);
+}
+
+static KernelFn fill_kernel(int algo) {
+  if (algo == kBFS) return k_fill<kBFS>;
+  if (algo == kSSSP) return k_fill<kSSSP>;
+  return k_fill<kCC>;
+}
+static KernelFn seed_kernel(int algo) {
+  if (algo == kBFS) return k_seed<kBFS>;
+  if (algo == kSSSP) return k_seed<kSSSP>;
+  return k_seed<kCC>;
+}
+
+// ---------------------------------------------------------------------------
+// Device state helpers.
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return I2_OK;
+  if (e == cudaErrorMemoryAllocation) return I2_ERR_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return I2_ERR_NO_DEVICE;
+  return I2_ERR_CUDA;
+}
+
+#define I2_CK(call)                         \
+  do {                                      \
+    cudaError_t e_ = (call);                \
+    if (e_ != cudaSuccess) {                \
+      cudaGetLastError();                   \
+      return cuda_status(e_);               \
+    }                                       \
+  } while (0)
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+int grid_for(KernelFn fn, int max_per_sm) {
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, kBlock, 0);
+  per = std::max(1, std::min(per, max_per_sm));
+  return per * sm_count();
+}
+
+// Per-device selector parameters.
+static std::mutex g_mlp_mu;
+static float* g_mlp_dev[64] = {nullptr};
+
+const float* mlp_device_params() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_mlp_mu);
+  return (dev >= 0 && dev < 64) ? g_mlp_dev[dev] : nullptr;
+}
+
+int mlp_install(const float* params, int count) {
+  if (!params || count != kParams) return I2_ERR_ARG;
+  int dev = 0;
+  I2_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return I2_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_mlp_mu);
+  if (!g_mlp_dev[dev]) I2_CK(cudaMalloc(&g_mlp_dev[dev], sizeof(float) * kParams));
+  I2_CK(cudaMemcpy(g_mlp_dev[dev], params, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+  return I2_OK;
+}
+
+}  // namespace i2
+
+using namespace i2;
+
+// ---------------------------------------------------------------------------
+// Graph handle.
+
+struct ExecKey {
+  int algo, mode, variant, multi;
+  bool operator<(const ExecKey& o) const {
+    if (algo != o.algo) return algo < o.algo;
+    if (mode != o.mode) return mode < o.mode;
+    if (variant != o.variant) return variant < o.variant;
+    return multi < o.multi;
+  }
+};
+
+struct ExecEntry {
+  cudaGraphExec_t ex = nullptr;
+  cudaGraphNode_t reset = nullptr;
+  RunParams last{};
+  Ctx ctx{};
+};
+
+struct i2_graph {
+  DGraph g{};
+  GStats gs{};
+  int device = 0;
+  bool owns = false;
+  int* d_nindex = nullptr;
+  int* d_nlist = nullptr;
+  int* d_eweight = nullptr;
+  bool owns_weights = false;
+  int* d_sp = nullptr;
+  int heavy = 4096;
+  int blocks_per_sm = 4;
+  // workspace
+  bool ws_ready = false;
+  int* dist = nullptr;
+  int* wl[3] = {nullptr, nullptr, nullptr};
+  int* hwl[3] = {nullptr, nullptr, nullptr};
+  unsigned* bm[3] = {nullptr, nullptr, nullptr};
+  int bm_words = 0;
+  Ctl* ctl = nullptr;
+  IterRec* recs = nullptr;
+  int rec_cap = 0;
+  int* srcs = nullptr;
+  int srcs_cap = 0;
+  unsigned long long* reach = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  Ctl* h_ctl = nullptr;  // pinned
+  std::map<ExecKey, ExecEntry> execs;
+  std::vector<cudaGraph_t> graphs;
+  int last_iters = 0;
+  // sweep scratch
+  int* snap_dist = nullptr;
+  unsigned* snap_bm = nullptr;
+  int* snap_wl = nullptr;
+  int* snap_hwl = nullptr;
+};
+
+namespace i2 {
+
+static void drop_execs(i2_graph* g) {
+  for (auto& kv : g->execs) cudaGraphExecDestroy(kv.second.ex);
+  g->execs.clear();
+}
+
+static void free_graph_state(i2_graph* g) {
+  drop_execs(g);
+  for (auto gr : g->graphs) cudaGraphDestroy(gr);
+  g->graphs.clear();
+  cudaFree(g->dist);
+  for (int k = 0; k < 3; ++k) {
+    cudaFree(g->wl[k]);
+    cudaFree(g->hwl[k]);
+  }
+  cudaFree(g->bm[0]);
+  cudaFree(g->ctl);
+  cudaFree(g->recs);
+  cudaFree(g->srcs);
+  cudaFree(g->reach);
+  cudaFree(g->snap_dist);
+  cudaFree(g->snap_bm);
+  cudaFree(g->snap_wl);
+  cudaFree(g->snap_hwl);
+  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->ev2) cudaEventDestroy(g->ev2);
+  if (g->ev3) cudaEventDestroy(g->ev3);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  cudaFree(g->d_sp);
+  if (g->owns) {
+    cudaFree(g->d_nindex);
+    cudaFree(g->d_nlist);
+  }
+  if (g->owns || g->owns_weights) cudaFree(g->d_eweight);
+}
+
+static int compute_stats(i2_graph* g) {
+  DevStats* st = nullptr;
+  I2_CK(cudaMalloc(&st, sizeof(DevStats)));
+  DevStats h{};
+  h.wmin = INT_MAX;
+  cudaMemcpy(st, &h, sizeof(h), cudaMemcpyHostToDevice);
+  const int grid = 4 * sm_count();
+  k_degree_stats<<<grid, 256, 0, g->stream>>>(g->g, g->heavy, st);
+  cudaStreamSynchronize(g->stream);
+  cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost);
+  if (!h.unsorted) {
+    k_symmetry<<<grid, 256, 0, g->stream>>>(g->g, st);
+    cudaStreamSynchronize(g->stream);
+    int asym = 0;
+    cudaMemcpy(&asym, &st->asym, sizeof(int), cudaMemcpyDeviceToHost);
+    h.asym = asym;
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaFree(st);
+  if (e != cudaSuccess) return cuda_status(e);
+  GStats& s = g->gs;
+  s.nodes = g->g.nodes;
+  s.edges = g->g.edges;
+  s.maxdeg = h.maxdeg;
+  s.nheavy = h.nheavy;
+  s.wmin = g->g.eweight ? (h.wmin == INT_MAX ? 1 : h.wmin) : 1;
+  s.symmetric = (!h.unsorted && !h.asym) ? 1 : 0;
+  const double mean = (double)g->g.edges / (double)g->g.nodes;
+  const double var = std::max(0.0, h.sumsq / (double)g->g.nodes - mean * mean);
+  s.avgdeg = (float)mean;
+  s.degcv = mean > 0 ? (float)(std::sqrt(var) / mean) : 0.f;
+  return I2_OK;
+}
+
+static int finish_setup(i2_graph* g) {
+  I2_CK(cudaGetDevice(&g->device));
+  I2_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  I2_CK(cudaEventCreate(&g->ev0));
+  I2_CK(cudaEventCreate(&g->ev1));
+  I2_CK(cudaEventCreate(&g->ev2));
+  I2_CK(cudaEventCreate(&g->ev3));
+  I2_CK(cudaMallocHost(&g->h_ctl, sizeof(Ctl)));
+  g->g.vec_ok = ((((uintptr_t)g->g.nlist) & 15) == 0 && (((uintptr_t)g->g.eweight) & 15) == 0) ? 1 : 0;
+  return compute_stats(g);
+}
+
+static int ensure_workspace(i2_graph* g) {
+  if (g->ws_ready) return I2_OK;
+  const long long V = g->g.nodes;
+  g->bm_words = (int)((V + 31) / 32);
+  I2_CK(cudaMalloc(&g->dist, sizeof(int) * V));
+  for (int k = 0; k < 3; ++k) {
+    I2_CK(cudaMalloc(&g->wl[k], sizeof(int) * V));
+    I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+  }
+  unsigned* bm = nullptr;
+  I2_CK(cudaMalloc(&bm, sizeof(unsigned) * 3ull * g->bm_words));
+  for (int k = 0; k < 3; ++k) g->bm[k] = bm + (size_t)k * g->bm_words;
+  I2_CK(cudaMalloc(&g->ctl, sizeof(Ctl)));
+  g->rec_cap = (int)std::min<long long>(V + 2, 1 << 16);
+  I2_CK(cudaMalloc(&g->recs, sizeof(IterRec) * g->rec_cap));
+  I2_CK(cudaMalloc(&g->reach, sizeof(unsigned long long) * 2));
+  g->ws_ready = true;
+  return I2_OK;
+}
+
+static int ensure_sp(i2_graph* g) {
+  if (g->d_sp) return I2_OK;
+  I2_CK(cudaMalloc(&g->d_sp, sizeof(int) * ((size_t)g->g.edges + 4)));
+  k_build_sp<<<8 * sm_count(), 256, 0, g->stream>>>(g->g, g->d_sp);
+  I2_CK(cudaStreamSynchronize(g->stream));
+  g->g.sp = g->d_sp;
+  return I2_OK;
+}
+
+static int allowed_mask(const i2_graph* g) {
+  int m = 0;
+  for (int v = 0; v < kNumVariants; ++v) m |= 1 << v;
+  if (!g->gs.symmetric) m &= ~((1 << kPullFrontier) | (1 << kPullTopo));
+  if (!g->d_sp) m &= ~(1 << kEdgeTopo);
+  return m;
+}
+
+static Ctx make_ctx(const i2_graph* g) {
+  Ctx c{};
+  c.g = g->g;
+  c.gs = g->gs;
+  c.dist = g->dist;
+  for (int k = 0; k < 3; ++k) {
+    c.wl[k] = g->wl[k];
+    c.hwl[k] = g->hwl[k];
+    c.bm[k] = g->bm[k];
+  }
+  c.ctl = g->ctl;
+  c.recs = g->recs;
+  c.rec_cap = g->rec_cap;
+  c.heavy = g->heavy;
+  c.bm_words = g->bm_words;
+  c.mlp = mlp_device_params();
+  c.srcs = nullptr;
+  return c;
+}
+
+static RunParams make_params(const i2_graph* g, int algo, int mode, int variant, int src, int nsrc, int cap) {
+  RunParams p;
+  p.algo = algo;
+  p.mode = mode;
+  p.fixed_variant = variant < 0 ? 0 : variant;
+  p.allowed = allowed_mask(g);
+  p.src = src;
+  p.nsrc = nsrc;
+  p.iter_cap = cap > 0 ? cap : g->g.nodes + 2;
+  return p;
+}
+
+static int add_kernel_node(cudaGraph_t gr, cudaGraphNode_t* node, const cudaGraphNode_t* deps, int ndeps,
+                           KernelFn fn, int grid, Ctx* ctx) {
+  cudaKernelNodeParams p{};
+  p.func = (void*)fn;
+  p.gridDim = dim3(grid);
+  p.blockDim = dim3(kBlock);
+  p.sharedMemBytes = 0;
+  void* args[1] = {ctx};
+  p.kernelParams = args;
+  p.extra = nullptr;
+  I2_CK(cudaGraphAddKernelNode(node, gr, deps, ndeps, &p));
+  return I2_OK;
+}
+
+static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, const RunParams& rp,
+                      ExecEntry** out) {
+  ExecKey key{algo, mode, mode == 0 ? variant : -1, multi ? 1 : 0};
+  auto it = g->execs.find(key);
+  if (it != g->execs.end()) {
+    *out = &it->second;
+    return I2_OK;
+  }
+  cudaGraph_t gr;
+  I2_CK(cudaGraphCreate(&gr, 0));
+  g->graphs.push_back(gr);
+  cudaGraphConditionalHandle loop_h, sw_h = 0;
+  I2_CK(cudaGraphConditionalHandleCreate(&loop_h, gr, 1, cudaGraphCondAssignDefault));
+  const bool sw = mode != 0;
+  if (sw) I2_CK(cudaGraphConditionalHandleCreate(&sw_h, gr, 0, cudaGraphCondAssignDefault));
+  Ctx c = make_ctx(g);
+  c.srcs = multi ? g->srcs : nullptr;
+  c.loop_h = (unsigned long long)loop_h;
+  c.switch_h = (unsigned long long)sw_h;
+  c.use_loop = 1;
+  c.use_switch = sw ? 1 : 0;
+  // bitmaps <- 0
+  cudaGraphNode_t n_ms, n_reset, n_fill, n_seed, n_loop;
+  cudaMemsetParams ms{};
+  ms.dst = g->bm[0];
+  ms.value = 0;
+  ms.elementSize = 4;
+  ms.width = 3ull * g->bm_words;
+  ms.height = 1;
+  ms.pitch = 0;
+  I2_CK(cudaGraphAddMemsetNode(&n_ms, gr, nullptr, 0, &ms));
+  // control block <- run parameters
+  {
+    cudaKernelNodeParams kp{};
+    Ctl* ctl = g->ctl;
+    RunParams p = rp;
+    void* args[2] = {&ctl, &p};
+    kp.func = (void*)k_reset;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    I2_CK(cudaGraphAddKernelNode(&n_reset, gr, &n_ms, 1, &kp));
+  }
+  int st = add_kernel_node(gr, &n_fill, &n_reset, 1, fill_kernel(algo), grid_for(fill_kernel(algo), 8), &c);
+  if (st) return st;
+  st = add_kernel_node(gr, &n_seed, &n_fill, 1, seed_kernel(algo), 1, &c);
+  if (st) return st;
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = loop_h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  I2_CK(cudaGraphAddNode(&n_loop, gr, &n_seed, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (!sw) {
+    cudaGraphNode_t n;
+    KernelFn fn = relax_kernel(algo, variant);
+    st = add_kernel_node(body, &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
+    if (st) return st;
+  } else {
+    cudaGraphNodeParams sp{};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = sw_h;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = kNumVariants;
+    cudaGraphNode_t n_sw;
+    I2_CK(cudaGraphAddNode(&n_sw, body, nullptr, 0, &sp));
+    for (int v = 0; v < kNumVariants; ++v) {
+      cudaGraphNode_t n;
+      KernelFn fn = relax_kernel(algo, v);
+      st = add_kernel_node(sp.conditional.phGraph_out[v], &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
+      if (st) return st;
+    }
+  }
+  ExecEntry e;
+  I2_CK(cudaGraphInstantiate(&e.ex, gr, 0));
+  e.reset = n_reset;
+  e.last = rp;
+  e.ctx = c;
+  auto ins = g->execs.emplace(key, e);
+  *out = &ins.first->second;
+  return I2_OK;
+}
+
+// Launch the traversal graph with this run's parameters. Changing the reset
+// node's arguments affects only launches made after the change.
+static int launch_exec(i2_graph* g, ExecEntry* e, const RunParams& rp, cudaStream_t s) {
+  if (e->last != rp) {
+    cudaKernelNodeParams kp{};
+    Ctl* ctl = g->ctl;
+    RunParams p = rp;
+    void* args[2] = {&ctl, &p};
+    kp.func = (void*)k_reset;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    I2_CK(cudaGraphExecKernelNodeSetParams(e->ex, e->reset, &kp));
+    e->last = rp;
+  }
+  I2_CK(cudaGraphLaunch(e->ex, s));
+  return I2_OK;
+}
+
+// Reset the bitmaps and the control block on the stream (host-driven paths).
+static int prepare_run(i2_graph* g, cudaStream_t s, const RunParams& rp) {
+  I2_CK(cudaMemsetAsync(g->bm[0], 0, sizeof(unsigned) * 3ull * g->bm_words, s));
+  k_reset<<<1, 32, 0, s>>>(g->ctl, rp);
+  I2_CK(cudaGetLastError());
+  return I2_OK;
+}
+
+// Host-driven loop (one control-block read per iteration, like the reference's
+// do-while). Each relax launch is bracketed by CUDA events on the launching
+// stream; their sum is returned in *relax_ms.
+static int run_host_loop(i2_graph* g, cudaStream_t s, int algo, bool multi, double* relax_ms) {
+  Ctx c = make_ctx(g);
+  c.srcs = multi ? g->srcs : nullptr;
+  KernelFn ff = fill_kernel(algo);
+  ff<<<grid_for(ff, 8), kBlock, 0, s>>>(c);
+  seed_kernel(algo)<<<1, kBlock, 0, s>>>(c);
+  Ctl* h = g->h_ctl;
+  double total = 0.0;
+  for (;;) {
+    I2_CK(cudaMemcpyAsync(h, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    I2_CK(cudaStreamSynchronize(s));
+    const int cur = h->iter % 3;
+    const long long n = (long long)h->slot[cur].size + h->slot[cur].hsize;
+    if (n == 0 || (h->status & kStatusIterCap)) break;
+    KernelFn fn = relax_kernel(algo, h->variant);
+    I2_CK(cudaEventRecord(g->ev2, s));
+    fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
+    I2_CK(cudaGetLastError());
+    I2_CK(cudaEventRecord(g->ev3, s));
+    I2_CK(cudaEventSynchronize(g->ev3));
+    float ms = 0.f;
+    I2_CK(cudaEventElapsedTime(&ms, g->ev2, g->ev3));
+    total += ms;
+  }
+  *relax_ms = total;
+  return I2_OK;
+}
+
+static int fill_report(i2_graph* g, cudaStream_t s, int algo, i2_report* rep, double host_relax_ms) {
+  I2_CK(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  I2_CK(cudaMemsetAsync(g->reach, 0, sizeof(unsigned long long) * 2, s));
+  k_reached<<<4 * sm_count(), 256, 0, s>>>(g->g, g->dist, g->reach);
+  unsigned long long r[2] = {0, 0};
+  I2_CK(cudaMemcpyAsync(r, g->reach, sizeof(r), cudaMemcpyDeviceToHost, s));
+  I2_CK(cudaStreamSynchronize(s));
+  const Ctl* h = g->h_ctl;
+  g->last_iters = h->iter;
+  if (rep) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    rep->seconds = ms * 1e-3;
+    rep->relax_seconds = host_relax_ms >= 0.0 ? host_relax_ms * 1e-3 : h->relax_ns * 1e-9;
+    rep->iterations = h->iter;
+    for (int k = 0; k < 16; ++k) rep->variant_hist[k] = h->hist[k];
+    rep->reached_vertices = (long long)r[0];
+    rep->reached_edges = (long long)r[1];
+  }
+  if (h->status & kStatusIterCap) return I2_ERR_ITER_CAP;
+  (void)algo;
+  return I2_OK;
+}
+
+int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
+                  i2_report* rep) {
+  if (!g) return I2_ERR_ARG;
+  if (algo < I2_BFS || algo > I2_CC) return I2_ERR_ARG;
+  I2_CK(cudaSetDevice(g->device));
+  i2_opts o{};
+  if (opts) o = *opts;
+  if (algo != I2_CC && !srcs_host && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
+  if (algo == I2_SSSP) {
+    if (!g->g.eweight) return I2_ERR_ARG;
+    if (g->gs.wmin < 0) return I2_ERR_UNSUPPORTED;
+  }
+  int st = ensure_workspace(g);
+  if (st) return st;
+  int mode = 0, variant = o.variant;
+  if (variant == I2_AUTO_HEURISTIC) mode = 1;
+  else if (variant == I2_AUTO_LEARNED) mode = 2;
+  else if (variant < 0 || variant >= kNumVariants) return I2_ERR_ARG;
+  if (mode != 0 || variant == kEdgeTopo) {
+    st = ensure_sp(g);
+    if (st) return st;
+  }
+  if (mode == 0 && !((allowed_mask(g) >> variant) & 1)) return I2_ERR_UNSUPPORTED;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
+  const bool multi = srcs_host != nullptr;
+  if (multi) {
+    if (nsrc < 1) return I2_ERR_ARG;
+    for (int j = 0; j < nsrc; ++j)
+      if (srcs_host[j] < 0 || srcs_host[j] >= g->g.nodes) return I2_ERR_ARG;
+    if (g->srcs_cap < nsrc) {
+      cudaFree(g->srcs);
+      g->srcs = nullptr;
+      I2_CK(cudaMalloc(&g->srcs, sizeof(int) * nsrc));
+      g->srcs_cap = nsrc;
+      // graphs bake the source pointer: rebuild them
+      drop_execs(g);
+    }
+    I2_CK(cudaMemcpyAsync(g->srcs, srcs_host, sizeof(int) * nsrc, cudaMemcpyHostToDevice, s));
+  }
+  const RunParams rp = make_params(g, algo, mode, variant, src, nsrc, o.iter_cap);
+  ExecEntry* ex = nullptr;
+  if (o.loop_mode == I2_LOOP_GRAPH) {
+    st = build_exec(g, algo, mode, variant, multi, rp, &ex);
+    if (st) return st;
+  }
+  double host_relax_ms = -1.0;
+  if (rep) I2_CK(cudaEventRecord(g->ev0, s));
+  if (o.loop_mode == I2_LOOP_GRAPH) {
+    st = launch_exec(g, ex, rp, s);
+    if (st) return st;
+  } else {
+    st = prepare_run(g, s, rp);
+    if (st) return st;
+    st = run_host_loop(g, s, algo, multi, &host_relax_ms);
+    if (st) return st;
+  }
+  if (rep) I2_CK(cudaEventRecord(g->ev1, s));
+  I2_CK(cudaGetLastError());
+  // Without a report the call stays asynchronous on the stream.
+  if (!rep && o.loop_mode == I2_LOOP_GRAPH) return I2_OK;
+  return fill_report(g, s, algo, rep, host_relax_ms);
+}
+
+int graph_adopt(int nodes, int edges, int* d_nindex, int* d_nlist, int* d_eweight, i2_graph** out) {
+  i2_graph* g = new i2_graph();
+  g->owns = true;
+  g->d_nindex = d_nindex;
+  g->d_nlist = d_nlist;
+  g->d_eweight = d_eweight;
+  g->g.nodes = nodes;
+  g->g.edges = edges;
+  g->g.nindex = d_nindex;
+  g->g.nlist = d_nlist;
+  g->g.eweight = d_eweight;
+  int st = finish_setup(g);
+  if (st) {
+    free_graph_state(g);
+    delete g;
+    return st;
+  }
+  *out = g;
+  return I2_OK;
+}
+
+int graph_copy_result(i2_graph* g, int* host_out, const i2_opts* opts) {
+  cudaStream_t s = (opts && opts->stream) ? (cudaStream_t)opts->stream : g->stream;
+  I2_CK(cudaMemcpyAsync(host_out, g->dist, sizeof(int) * (size_t)g->g.nodes, cudaMemcpyDeviceToHost, s));
+  I2_CK(cudaStreamSynchronize(s));
+  return I2_OK;
+}
+
+// Per-iteration sweep: along the trajectory of `follow` (a variant, or the
+// heuristic when negative), save the state before each launch, time every
+// allowed variant from that state (best of `reps`), restore, and advance.
+static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_record* recs, float* times, int cap,
+                 int* nout) {
+  I2_CK(cudaSetDevice(g->device));
+  int st = ensure_workspace(g);
+  if (st) return st;
+  st = ensure_sp(g);
+  if (st) return st;
+  const long long V = g->g.nodes;
+  if (!g->snap_dist) {
+    I2_CK(cudaMalloc(&g->snap_dist, sizeof(int) * V));
+    I2_CK(cudaMalloc(&g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words));
+  }
+  cudaStream_t s = g->stream;
+  const int mode = follow < 0 ? 1 : 0;
+  st = prepare_run(g, s, make_params(g, algo, mode, follow < 0 ? 0 : follow, src, 1, 0));
+  if (st) return st;
+  Ctx c = make_ctx(g);
+  KernelFn ff = fill_kernel(algo);
+  ff<<<grid_for(ff, 8), kBlock, 0, s>>>(c);
+  seed_kernel(algo)<<<1, kBlock, 0, s>>>(c);
+  const int allowed = allowed_mask(g);
+  Ctl snap;
+  int it = 0;
+  for (; it < cap; ++it) {
+    I2_CK(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    I2_CK(cudaStreamSynchronize(s));
+    snap = *g->h_ctl;
+    const int cur = snap.iter % 3;
+    if ((long long)snap.slot[cur].size + snap.slot[cur].hsize == 0) break;
+    I2_CK(cudaMemcpyAsync(g->snap_dist, g->dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
+    I2_CK(cudaMemcpyAsync(g->snap_bm, g->bm[0], sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
+    for (int v = 0; v < kNumVariants; ++v) {
+      float best = -1.f;
+      if ((allowed >> v) & 1) {
+        KernelFn fn = relax_kernel(algo, v);
+        const int grid = grid_for(fn, g->blocks_per_sm);
+        for (int r = 0; r < std::max(1, reps); ++r) {
+          *g->h_ctl = snap;
+          I2_CK(cudaMemcpyAsync(g->ctl, g->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+          I2_CK(cudaMemcpyAsync(g->dist, g->snap_dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
+          I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
+          I2_CK(cudaEventRecord(g->ev0, s));
+          fn<<<grid, kBlock, 0, s>>>(c);
+          I2_CK(cudaEventRecord(g->ev1, s));
+          I2_CK(cudaEventSynchronize(g->ev1));
+          float ms = 0.f;
+          I2_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+          if (best < 0.f || ms < best) best = ms;
+        }
+        best *= 1e6f;  // ns
+      }
+      times[(size_t)it * kNumVariants + v] = best;
+    }
+    *g->h_ctl = snap;
+    I2_CK(cudaMemcpyAsync(g->ctl, g->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    I2_CK(cudaMemcpyAsync(g->dist, g->snap_dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
+    I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
+    KernelFn fn = relax_kernel(algo, snap.variant);
+    fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
+    I2_CK(cudaGetLastError());
+    if (snap.iter < g->rec_cap)
+      I2_CK(cudaMemcpyAsync(&recs[it], g->recs + snap.iter, sizeof(IterRec), cudaMemcpyDeviceToHost, s));
+  }
+  I2_CK(cudaStreamSynchronize(s));
+  *nout = it;
+  g->last_iters = it;
+  return I2_OK;
+}
+
+}  // namespace i2
+
+// ---------------------------------------------------------------------------
+// C ABI.
+
+extern "C" {
+
+const char* i2_status_string(int status) {
+  switch (status) {
+    case I2_OK: return "ok";
+    case I2_ERR_ARG: return "invalid argument";
+    case I2_ERR_IO: return "file i/o error";
+    case I2_ERR_FORMAT: return "malformed graph";
+    case I2_ERR_NOMEM: return "out of memory";
+    case I2_ERR_CUDA: return "cuda error";
+    case I2_ERR_NO_DEVICE: return "no cuda device";
+    case I2_ERR_UNSUPPORTED: return "variant not supported on this graph";
+    case I2_ERR_ITER_CAP: return "iteration cap reached";
+    case I2_ERR_OVERFLOW: return "int32 limit exceeded";
+  }
+  return "unknown status";
+}
+
+const char* i2_variant_name(int v) {
+  static const char* names[] = {"vp_thread", "vp_warp", "vp_cta", "vp_block",
+                                "pull_frontier", "pull_topo", "edge_topo", "push_topo"};
+  if (v == I2_AUTO_HEURISTIC) return "auto_heuristic";
+  if (v == I2_AUTO_LEARNED) return "auto_learned";
+  if (v < 0 || v >= kNumVariants) return "invalid";
+  return names[v];
+}
+
+int i2_version(void) { return 100; }
+
+int i2_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+static int upload_common(i2_graph* g) {
+  int st = finish_setup(g);
+  if (st) {
+    free_graph_state(g);
+    delete g;
+  }
+  return st;
+}
+
+int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
+  if (!h || !out) return I2_ERR_ARG;
+  *out = nullptr;
+  int st = validate_host_csr(h);
+  if (st) return st;
+  if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
+  i2_graph* g = new i2_graph();
+  g->owns = true;
+  const size_t nn = (size_t)h->nodes + 1, ne = (size_t)h->edges + 4;
+  cudaError_t e = cudaMalloc(&g->d_nindex, sizeof(int) * nn);
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_nlist, sizeof(int) * ne);
+  if (e == cudaSuccess && h->eweight) e = cudaMalloc(&g->d_eweight, sizeof(int) * ne);
+  if (e == cudaSuccess) e = cudaMemcpy(g->d_nindex, h->nindex, sizeof(int) * nn, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(g->d_nlist, h->nlist, sizeof(int) * h->edges, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && h->eweight)
+    e = cudaMemcpy(g->d_eweight, h->eweight, sizeof(int) * h->edges, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    free_graph_state(g);
+    delete g;
+    return cuda_status(e);
+  }
+  g->g.nodes = h->nodes;
+  g->g.edges = h->edges;
+  g->g.nindex = g->d_nindex;
+  g->g.nlist = g->d_nlist;
+  g->g.eweight = g->d_eweight;
+  st = upload_common(g);
+  if (st) return st;
+  *out = g;
+  return I2_OK;
+}
+
+int i2_graph_wrap_device(const i2_eclgraph* d, i2_graph** out) {
+  if (!d || !out || d->nodes < 1 || d->edges < 0 || !d->nindex || (d->edges > 0 && !d->nlist)) return I2_ERR_ARG;
+  *out = nullptr;
+  if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
+  i2_graph* g = new i2_graph();
+  g->owns = false;
+  g->d_nindex = d->nindex;
+  g->d_nlist = d->nlist;
+  g->d_eweight = d->eweight;
+  g->g.nodes = d->nodes;
+  g->g.edges = d->edges;
+  g->g.nindex = d->nindex;
+  g->g.nlist = d->nlist;
+  g->g.eweight = d->eweight;
+  // Validate before any kernel indexes through the arrays.
+  int* bad = nullptr;
+  int hbad = 0;
+  cudaError_t e = cudaMalloc(&bad, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(bad, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_validate<<<4 * sm_count(), 256>>>(g->g, bad);
+    e = cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(bad);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete g;
+    return cuda_status(e);
+  }
+  if (hbad) {
+    delete g;
+    return I2_ERR_FORMAT;
+  }
+  int st = upload_common(g);
+  if (st) return st;
+  *out = g;
+  return I2_OK;
+}
+
+int i2_graph_info_get(const i2_graph* g, i2_graph_info* out) {
+  if (!g || !out) return I2_ERR_ARG;
+  out->nodes = g->gs.nodes;
+  out->edges = g->gs.edges;
+  out->maxdeg = g->gs.maxdeg;
+  out->nheavy = g->gs.nheavy;
+  out->wmin = g->gs.wmin;
+  out->symmetric = g->gs.symmetric;
+  out->has_weights = g->g.eweight != nullptr;
+  out->avgdeg = g->gs.avgdeg;
+  out->degcv = g->gs.degcv;
+  return I2_OK;
+}
+
+int i2_graph_download(const i2_graph* g, i2_eclgraph* out) {
+  if (!g || !out) return I2_ERR_ARG;
+  int st = i2_alloc_eclgraph(g->g.nodes, g->g.edges, g->g.eweight ? 1 : 0, out);
+  if (st) return st;
+  cudaError_t e = cudaMemcpy(out->nindex, g->g.nindex, sizeof(int) * ((size_t)g->g.nodes + 1), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out->nlist, g->g.nlist, sizeof(int) * (size_t)g->g.edges, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && g->g.eweight)
+    e = cudaMemcpy(out->eweight, g->g.eweight, sizeof(int) * (size_t)g->g.edges, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    i2_free_eclgraph(out);
+    return cuda_status(e);
+  }
+  return I2_OK;
+}
+
+int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm) {
+  if (!g || heavy_threshold < 0 || blocks_per_sm < 0 || blocks_per_sm > 32) return I2_ERR_ARG;
+  I2_CK(cudaSetDevice(g->device));
+  if (g->stream) I2_CK(cudaStreamSynchronize(g->stream));
+  drop_execs(g);
+  if (blocks_per_sm) g->blocks_per_sm = blocks_per_sm;
+  if (heavy_threshold && heavy_threshold != g->heavy) {
+    g->heavy = std::max(32, heavy_threshold);
+    // the heavy lists are sized by the number of heavy vertices
+    for (int k = 0; k < 3; ++k) {
+      cudaFree(g->hwl[k]);
+      g->hwl[k] = nullptr;
+    }
+    int st = compute_stats(g);
+    if (st) return st;
+    if (g->ws_ready)
+      for (int k = 0; k < 3; ++k) I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+  }
+  return I2_OK;
+}
+
+int i2_graph_synth_weights(i2_graph* g) {
+  if (!g) return I2_ERR_ARG;
+  if (g->g.eweight) return I2_OK;
+  I2_CK(cudaSetDevice(g->device));
+  int* w = nullptr;
+  I2_CK(cudaMalloc(&w, sizeof(int) * ((size_t)g->g.edges + 4)));
+  k_synth_weights<<<8 * sm_count(), 256, 0, g->stream>>>(g->g, w);
+  I2_CK(cudaStreamSynchronize(g->stream));
+  g->d_eweight = w;
+  g->owns_weights = true;
+  g->g.eweight = w;
+  g->g.vec_ok = ((((uintptr_t)g->g.nlist) & 15) == 0 && (((uintptr_t)w) & 15) == 0) ? 1 : 0;
+  drop_execs(g);
+  return compute_stats(g);
+}
+
+int i2_graph_free(i2_graph* g) {
+  if (!g) return I2_ERR_ARG;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  free_graph_state(g);
+  delete g;
+  return I2_OK;
+}
+
+static int run_host_out(i2_graph* g, int algo, int src, int* out, const i2_opts* opts, i2_report* rep) {
+  if (!out) return I2_ERR_ARG;
+  int st = run_traversal(g, algo, src, nullptr, 0, opts, rep);
+  if (st && st != I2_ERR_ITER_CAP) return st;
+  cudaStream_t s = (opts && opts->stream) ? (cudaStream_t)opts->stream : g->stream;
+  I2_CK(cudaMemcpyAsync(out, g->dist, sizeof(int) * (size_t)g->g.nodes, cudaMemcpyDeviceToHost, s));
+  I2_CK(cudaStreamSynchronize(s));
+  return st;
+}
+
+int i2_bfs(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep) {
+  return run_host_out(g, I2_BFS, src, dist, opts, rep);
+}
+int i2_sssp(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep) {
+  return run_host_out(g, I2_SSSP, src, dist, opts, rep);
+}
+int i2_cc(i2_graph* g, int* label, const i2_opts* opts, i2_report* rep) {
+  return run_host_out(g, I2_CC, 0, label, opts, rep);
+}
+
+int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* opts, i2_report* rep) {
+  int st = run_traversal(g, algo, algo == I2_CC ? 0 : src, nullptr, 0, opts, rep);
+  if (st && st != I2_ERR_ITER_CAP) return st;
+  if (out_dev) {
+    cudaStream_t s = (opts && opts->stream) ? (cudaStream_t)opts->stream : g->stream;
+    I2_CK(cudaMemcpyAsync(out_dev, g->dist, sizeof(int) * (size_t)g->g.nodes, cudaMemcpyDeviceToDevice, s));
+  }
+  return st;
+}
+
+int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n) {
+  if (!g || !out || !n || cap < 0) return I2_ERR_ARG;
+  if (!g->ws_ready) {
+    *n = 0;
+    return I2_OK;
+  }
+  const int m = std::min(std::min(g->last_iters, g->rec_cap), cap);
+  if (m > 0) I2_CK(cudaMemcpy(out, g->recs, sizeof(IterRec) * m, cudaMemcpyDeviceToHost));
+  *n = m;
+  return I2_OK;
+}
+
+int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_record* recs, float* times, int cap,
+             int* n) {
+  if (!g || !recs || !times || !n || cap < 1 || algo < I2_BFS || algo > I2_CC) return I2_ERR_ARG;
+  if (follow >= kNumVariants) return I2_ERR_ARG;
+  if (algo != I2_CC && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
+  if (algo == I2_SSSP && !g->g.eweight) return I2_ERR_ARG;
+  if (follow >= 0) {
+    int st = ensure_sp(g);
+    if (st) return st;
+    if (!((allowed_mask(g) >> follow) & 1)) return I2_ERR_UNSUPPORTED;
+  }
+  return sweep(g, algo, src, follow, reps, recs, times, cap, n);
+}
+
+int i2_mlp_param_count(void) { return kParams; }
+
+int i2_mlp_set_params(const float* params, int count) { return mlp_install(params, count); }
+
+}  // extern "C"

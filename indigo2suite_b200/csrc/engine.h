@@ -1,0 +1,29 @@
+// Internal interface between the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include "../../include/i2b200.h"
+#include "common.cuh"
+
+namespace i2 {
+
+typedef void (*KernelFn)(Ctx);
+
+int cuda_status(cudaError_t e);
+int grid_for(KernelFn fn, int max_per_sm);
+KernelFn relax_kernel(int algo, int variant);
+const float* mlp_device_params();
+int mlp_install(const float* params, int count);
+
+// One traversal of a device graph from one source (srcs_host == nullptr) or
+// from nsrc sources at once (batched graphs). The result stays in the graph's
+// workspace.
+int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
+                  i2_report* rep);
+
+// Take ownership of CSR arrays already on the device and build a graph handle.
+int graph_adopt(int nodes, int edges, int* d_nindex, int* d_nlist, int* d_eweight, i2_graph** out);
+
+// Copy the last traversal's values to a host array of g.nodes ints.
+int graph_copy_result(i2_graph* g, int* host_out, const i2_opts* opts);
+
+}  // namespace i2

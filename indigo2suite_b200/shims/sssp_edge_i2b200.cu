@@ -1,0 +1,15 @@
+// Drop-in variant body for the Indigo2 harness include/sssp_edge_cuda.h,
+// implementing GPUsssp_edge(const int src, const ECLgraph& g, basic_t* const dist, const int* const sp) (include/sssp_edge_cuda.h:60) on libi2b200. See shim_common.h.
+#include <cuda/atomic>
+typedef int flag_t;
+typedef int data_type;
+typedef int basic_t;
+static const int ThreadsPerBlock = 512;
+#include "sssp_edge_cuda.h"
+#include "shim_common.h"
+
+static double GPUsssp_edge(const int src, const ECLgraph& g, basic_t* const dist, const int* const sp)
+{
+  (void)sp;  // the engine builds its own starting-point array on the device when needed
+  return i2shim_run(I2_SSSP, src, g.nodes, g.edges, g.nindex, g.nlist, g.eweight, dist, I2_VP_CTA);
+}

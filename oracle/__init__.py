@@ -1,0 +1,250 @@
+"""ORACLE — test infrastructure only.
+
+Checker for the engine's results: ctypes access to the C restatement in
+oracle.c (liboracle.so) and helpers that run the reference's own programs built
+by oracle/Makefile into oracle/_ref/ (the reference's serial Dijkstra, its
+OpenMP harness used as a verifier of injected results, its CPU programs and a
+few of its CUDA programs). Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg may use this package; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_OUT = HERE / "_ref"
+REFERENCE_ROOT = Path("/root/reference")
+
+_lib = None
+
+
+def build(ref: bool = True) -> None:
+    """Build liboracle.so, and the _ref/ programs when the reference tree is present."""
+    target = "all" if ref else "oracle"
+    subprocess.run(["make", "-s", "-C", str(HERE), target], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build(ref=False)
+        _lib = C.CDLL(str(path))
+        P = C.POINTER(C.c_int)
+        _lib.oracle_bfs.argtypes = [C.c_int, P, P, C.c_int, P]
+        _lib.oracle_sssp.argtypes = [C.c_int, P, P, P, C.c_int, P]
+        _lib.oracle_cc_minlabel.argtypes = [C.c_int, P, P, P]
+        _lib.oracle_cc_check.argtypes = [C.c_int, P, P, P]
+        _lib.oracle_synth_weights.argtypes = [C.c_int, P, P, P]
+        _lib.oracle_sp.argtypes = [C.c_int, P, P]
+        _lib.oracle_synth_weights.restype = None
+        _lib.oracle_sp.restype = None
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _csr(g):
+    return np.ascontiguousarray(g.nindex, np.int32), np.ascontiguousarray(g.nlist, np.int32)
+
+
+def bfs(g, src: int) -> np.ndarray:
+    ni, nl = _csr(g)
+    out = np.empty(g.nodes, np.int32)
+    rc = lib().oracle_bfs(g.nodes, _p(ni), _p(nl), src, _p(out))
+    assert rc == 0, rc
+    return out
+
+
+def sssp(g, src: int) -> np.ndarray:
+    ni, nl = _csr(g)
+    w = np.ascontiguousarray(g.eweight, np.int32)
+    out = np.empty(g.nodes, np.int32)
+    rc = lib().oracle_sssp(g.nodes, _p(ni), _p(nl), _p(w), src, _p(out))
+    assert rc == 0, rc
+    return out
+
+
+def cc(g) -> np.ndarray:
+    ni, nl = _csr(g)
+    out = np.empty(g.nodes, np.int32)
+    rc = lib().oracle_cc_minlabel(g.nodes, _p(ni), _p(nl), _p(out))
+    assert rc == 0, rc
+    return out
+
+
+def cc_check(g, label: np.ndarray) -> int:
+    ni, nl = _csr(g)
+    return int(lib().oracle_cc_check(g.nodes, _p(ni), _p(nl), _p(np.ascontiguousarray(label, np.int32))))
+
+
+def synth_weights(g) -> np.ndarray:
+    ni, nl = _csr(g)
+    w = np.empty(max(g.edges, 1), np.int32)
+    lib().oracle_synth_weights(g.nodes, _p(ni), _p(nl), _p(w))
+    return w[: g.edges]
+
+
+def sp(g) -> np.ndarray:
+    ni, _ = _csr(g)
+    out = np.empty(max(g.edges, 1), np.int32)
+    lib().oracle_sp(g.nodes, _p(ni), _p(out))
+    return out[: g.edges]
+
+
+# ---------------------------------------------------------------------------
+# The reference's own programs (oracle/_ref).
+
+def have_ref() -> bool:
+    return (REF_OUT / "libref_serial_bfs.so").exists()
+
+
+_serial = {}
+
+
+def ref_serial(kind: str, g, src: int) -> np.ndarray:
+    """The reference's CPUserialDijkstra from harness `kind` in {bfs, sssp_vertex, sssp_edge}."""
+    if kind not in _serial:
+        L = C.CDLL(str(REF_OUT / f"libref_serial_{kind}.so"))
+        P = C.POINTER(C.c_int)
+        L.ref_serial.argtypes = [C.c_int, C.c_int, P, P, P, C.c_int, P]
+        _serial[kind] = L
+    ni, nl = _csr(g)
+    w = np.ascontiguousarray(g.eweight, np.int32) if g.eweight is not None else None
+    out = np.empty(g.nodes, np.int32)
+    _serial[kind].ref_serial(g.nodes, g.edges, _p(ni), _p(nl), _p(w) if w is not None else None, src, _p(out))
+    return out
+
+
+def write_egr(g, path: str) -> None:
+    """ECLgraph file (include/ECLgraph.h:82-96 layout), written by numpy."""
+    with open(path, "wb") as f:
+        np.array([g.nodes, g.edges], np.int32).tofile(f)
+        np.ascontiguousarray(g.nindex, np.int32).tofile(f)
+        np.ascontiguousarray(g.nlist, np.int32).tofile(f)
+        if g.eweight is not None:
+            np.ascontiguousarray(g.eweight, np.int32).tofile(f)
+
+
+def ref_verify(kind: str, egr_path: str, values: np.ndarray, src: int | None = 0, timeout: float = 600) -> tuple[bool, str]:
+    """Run the reference harness `inject_<kind>` on the graph file with `values`
+    as the variant's result; True when the reference verifier passes."""
+    exe = REF_OUT / f"inject_{kind}"
+    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+        np.ascontiguousarray(values, np.int32).tofile(f)
+        rpath = f.name
+    try:
+        args = [str(exe), str(egr_path)] + ([str(src)] if src is not None else []) + ["1"]
+        env = dict(os.environ, I2_RESULT=rpath, OMP_NUM_THREADS="1")
+        p = subprocess.run(args, capture_output=True, text=True, env=env, timeout=timeout)
+        out = p.stdout + p.stderr
+        return (p.returncode == 0 and "verification passed" in out), out
+    finally:
+        os.unlink(rpath)
+
+
+def run_ref_program(name: str, args: list[str], threads: int | None = None, timeout: float = 900) -> dict:
+    """Run a reference program from _ref/ and parse its printed runtime/throughput."""
+    env = dict(os.environ)
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    p = subprocess.run([str(REF_OUT / name), *args], capture_output=True, text=True, env=env, timeout=timeout)
+    out = p.stdout + p.stderr
+    rt = re.findall(r"runtime:\s*([0-9.eE+-]+)\s*s", out)
+    tp = re.findall(r"Throughput:\s*([0-9.eE+-]+)\s*gigaedges/s", out)
+    return {"rc": p.returncode, "out": out, "runtime": float(rt[-1]) if rt else None,
+            "gteps": float(tp[-1]) if tp else None, "verified": "verification passed" in out}
+
+
+# ---------------------------------------------------------------------------
+# Size-independent certificates (vectorised numpy), for sizes where running
+# the serial oracle is too slow.
+
+def certify_distances(g, src: int, dist: np.ndarray, weighted: bool) -> str | None:
+    """Shortest-path certificate: dist[src] == 0; dist[v] <= dist[u] + w(u, v) on
+    every edge; every other reached vertex has a tight in-edge; unreached
+    vertices have no reached neighbour. Returns None when it holds."""
+    INF = np.iinfo(np.int32).max
+    d = np.asarray(dist, np.int64)
+    if d[src] != 0:
+        return "dist[src] != 0"
+    deg = np.diff(np.asarray(g.nindex, np.int64))
+    u = np.repeat(np.arange(g.nodes, dtype=np.int64), deg)
+    v = np.asarray(g.nlist, np.int64)
+    w = np.asarray(g.eweight, np.int64) if weighted else np.ones(g.edges, np.int64)
+    du, dv = d[u], d[v]
+    reached_u = du != INF
+    if (dv[reached_u] == INF).any():
+        return "unreached neighbour of a reached vertex"
+    cand = du + w
+    if (dv[reached_u] > cand[reached_u]).any():
+        return "relaxable edge"
+    tight = np.zeros(g.nodes, bool)
+    tv = v[reached_u & (dv == cand)]
+    tight[tv] = True
+    reached = d != INF
+    reached[src] = False
+    if not tight[reached].all():
+        return "reached vertex without a tight in-edge"
+    return None
+
+
+def certify_cc(g, label: np.ndarray) -> str | None:
+    """Minimum-label certificate on a symmetric graph: labels equal across every
+    edge, label[v] <= v, label[label[v]] == label[v], and as many distinct labels
+    as components (union-find in numpy by repeated min-propagation is avoided:
+    the count comes from scipy's connected_components)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    lab = np.asarray(label, np.int64)
+    deg = np.diff(np.asarray(g.nindex, np.int64))
+    u = np.repeat(np.arange(g.nodes, dtype=np.int64), deg)
+    if (lab[u] != lab[np.asarray(g.nlist, np.int64)]).any():
+        return "adjacent labels differ"
+    if (lab > np.arange(g.nodes)).any() or (lab < 0).any():
+        return "label above its vertex id"
+    if (lab[lab] != lab).any():
+        return "label is not its own label"
+    m = csr_matrix((np.ones(g.edges, np.int8), np.asarray(g.nlist), np.asarray(g.nindex)), shape=(g.nodes, g.nodes))
+    ncomp, _ = connected_components(m, directed=False)
+    if len(np.unique(lab)) != ncomp:
+        return "label count != component count"
+    return None
+
+
+# ---------------------------------------------------------------------------
+# One call of a reference CPU host driver (oracle/_ref/libref_cpu_<name>.so).
+
+_cpu = {}
+
+
+def ref_cpu_run(name: str, g, src: int, threads: int, sp: np.ndarray | None = None) -> tuple[float, np.ndarray]:
+    """Run the reference CPU program `name` (sssp_edge_cpp, sssp_vertex_cpp,
+    sssp_edge_omp, bfs_cpp, bfs_omp, cc_cpp, cc_omp) once; returns its own
+    measured runtime in seconds and the result."""
+    if name not in _cpu:
+        L = C.CDLL(str(REF_OUT / f"libref_cpu_{name}.so"))
+        P = C.POINTER(C.c_int)
+        L.ref_cpu_run.argtypes = [C.c_int, C.c_int, P, P, P, C.c_int, P, P, C.c_int]
+        L.ref_cpu_run.restype = C.c_double
+        _cpu[name] = L
+    ni, nl = _csr(g)
+    w = np.ascontiguousarray(g.eweight, np.int32) if g.eweight is not None else None
+    if sp is None and "edge" in name:
+        sp = globals()["sp"](g)
+    out = np.empty(g.nodes, np.int32)
+    t = _cpu[name].ref_cpu_run(g.nodes, g.edges, _p(ni), _p(nl), _p(w) if w is not None else None, src, _p(out),
+                               _p(sp) if sp is not None else None, threads)
+    return float(t), out

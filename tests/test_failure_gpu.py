@@ -1,0 +1,73 @@
+"""Failure handling that faults no GPU: every error is a status code."""
+import numpy as np
+import pytest
+
+import indigo2suite_b200 as i2
+from indigo2suite_b200 import _capi
+
+pytestmark = pytest.mark.gpu
+
+
+def test_iteration_cap_is_a_status(gpu):
+    # a path needs nodes - 1 iterations; cap it at 3
+    n = 50
+    nindex = np.concatenate([[0], np.cumsum([1] + [2] * (n - 2) + [1])]).astype(np.int32)
+    nl = []
+    for v in range(n):
+        if v > 0:
+            nl.append(v - 1)
+        if v < n - 1:
+            nl.append(v + 1)
+    g = i2.ECLGraph(n, len(nl), nindex, np.array(nl, np.int32), np.ones(len(nl), np.int32))
+    dg = i2.DeviceGraph.upload(g)
+    for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+        with pytest.raises(i2.I2Error) as e:
+            dg.bfs(0, iter_cap=3, loop=loop)
+        assert e.value.status == _capi.I2_ERR_ITER_CAP
+    # the context stays usable
+    d, rep = dg.bfs(0)
+    assert d[-1] == n - 1 and rep.iterations == n
+    dg.free()
+
+
+def test_bad_arguments(gpu):
+    g = i2.gen_er(100, 300, 2)
+    dg = i2.DeviceGraph.upload(g)
+    for src in (-1, 100):
+        with pytest.raises(i2.I2Error) as e:
+            dg.bfs(src)
+        assert e.value.status == _capi.I2_ERR_ARG
+    with pytest.raises(i2.I2Error):
+        dg.bfs(0, variant=99)
+    dg.free()
+    nw = i2.DeviceGraph.upload(i2.ECLGraph(g.nodes, g.edges, g.nindex, g.nlist, None))
+    with pytest.raises(i2.I2Error) as e:
+        nw.sssp(0)
+    assert e.value.status == _capi.I2_ERR_ARG
+    nw.synth_weights()  # the reference harness's weights, made on the device
+    ref = i2.synth_weights(i2.ECLGraph(g.nodes, g.edges, g.nindex, g.nlist, None))
+    np.testing.assert_array_equal(nw.download().eweight, ref.eweight)
+    import oracle
+    np.testing.assert_array_equal(nw.sssp(0)[0], oracle.sssp(ref, 0))
+    nw.free()
+
+
+def test_malformed_device_graph_rejected_before_any_traversal(gpu):
+    import torch
+
+    g = i2.gen_er(64, 128, 3)
+    ni = torch.tensor(g.nindex, dtype=torch.int32, device="cuda")
+    nl = torch.tensor(g.nlist, dtype=torch.int32, device="cuda")
+    ok = i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
+    assert np.array_equal(ok.bfs(0)[0], __import__("oracle").bfs(g, 0))
+    ok.free()
+    nl[5] = 1000  # out of range
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
+    assert e.value.status == _capi.I2_ERR_FORMAT
+    nl[5] = 1
+    ni[3] = ni[4] + 1  # non-monotone
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
+    assert e.value.status == _capi.I2_ERR_FORMAT
+    torch.cuda.synchronize()

@@ -1,0 +1,144 @@
+"""Host side of the library (no GPU): ECLgraph files, generators, C ABI surface."""
+import ctypes as C
+import os
+import re
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import indigo2suite_b200 as i2
+from indigo2suite_b200 import _capi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _is_symmetric_simple(g):
+    deg = g.degrees()
+    src = np.repeat(np.arange(g.nodes), deg)
+    assert (src != g.nlist).all(), "self-loop"
+    key = src.astype(np.int64) * g.nodes + g.nlist
+    assert len(np.unique(key)) == g.edges, "duplicate"
+    rkey = g.nlist.astype(np.int64) * g.nodes + src
+    assert np.array_equal(np.sort(key), np.sort(rkey)), "not symmetric"
+    for v in range(0, g.nodes, max(1, g.nodes // 97)):
+        a = g.nlist[g.nindex[v]:g.nindex[v + 1]]
+        assert (np.diff(a) > 0).all(), "unsorted adjacency"
+    if g.eweight is not None:
+        order = np.argsort(key)
+        rorder = np.argsort(rkey)
+        assert np.array_equal(g.eweight[order], g.eweight[rorder]), "weights not symmetric"
+        assert g.eweight.min() >= 1 and g.eweight.max() <= 255
+
+
+def test_er_exact_size_and_simple():
+    g = i2.gen_er(65536, 262144, 1)
+    assert g.nodes == 65536 and g.edges == 524288
+    _is_symmetric_simple(g)
+
+
+def test_generators_are_deterministic_and_seeded():
+    a = i2.gen_rmat(11, 16, seed=9)
+    b = i2.gen_rmat(11, 16, seed=9)
+    c = i2.gen_rmat(11, 16, seed=10)
+    assert np.array_equal(a.nlist, b.nlist) and np.array_equal(a.eweight, b.eweight)
+    assert not np.array_equal(a.nindex, c.nindex)
+    _is_symmetric_simple(a)
+
+
+def test_rmat_is_skewed_and_dedup_ratio():
+    g = i2.gen_rmat(14, 16, seed=1)
+    ratio = g.edges / (2 * 16 * g.nodes)
+    assert 0.8 < ratio < 0.95
+    assert g.degrees().max() > 50 * g.degrees().mean()
+
+
+def test_grid_shape():
+    side = 64
+    g = i2.gen_grid(side, 0.05, 0.001, 4)
+    _is_symmetric_simple(g)
+    full = 2 * 2 * side * (side - 1)
+    assert 0.9 * full < g.edges < full
+    assert g.degrees().max() <= 8
+
+
+def test_eclgraph_roundtrip_and_reference_layout(tmp_path):
+    g = i2.gen_rmat(8, 4, seed=2)
+    p = tmp_path / "g.egr"
+    i2.write_eclgraph(g, str(p))
+    raw = np.fromfile(p, np.int32)
+    assert raw[0] == g.nodes and raw[1] == g.edges
+    assert np.array_equal(raw[2:2 + g.nodes + 1], g.nindex)
+    assert np.array_equal(raw[3 + g.nodes:3 + g.nodes + g.edges], g.nlist)
+    assert np.array_equal(raw[3 + g.nodes + g.edges:], g.eweight)
+    h = i2.read_eclgraph(str(p))
+    assert np.array_equal(h.nindex, g.nindex) and np.array_equal(h.eweight, g.eweight)
+    # without weights: the reader reports none (include/ECLgraph.h:70-76)
+    q = tmp_path / "nw.egr"
+    i2.write_eclgraph(i2.ECLGraph(g.nodes, g.edges, g.nindex, g.nlist, None), str(q))
+    assert i2.read_eclgraph(str(q)).eweight is None
+
+
+def test_reads_reference_small_inputs(golden):
+    for name, case in golden.items():
+        g = case["graph"]
+        assert g.nindex[0] == 0 and g.nindex[-1] == g.edges
+
+
+@pytest.mark.parametrize("mutate,status", [
+    (lambda raw: raw[:1], _capi.I2_ERR_FORMAT),                       # header truncated
+    (lambda raw: raw[:5], _capi.I2_ERR_FORMAT),                       # nindex truncated
+    (lambda raw: np.concatenate([raw, raw[-3:-1]]), _capi.I2_ERR_FORMAT),  # partial weights
+    (lambda raw: np.concatenate([[0], raw[1:]]), _capi.I2_ERR_FORMAT),     # nodes < 1
+    (lambda raw: np.concatenate([raw[:1], [-1], raw[2:]]), _capi.I2_ERR_FORMAT),  # edges < 0
+])
+def test_malformed_files_are_status_codes(tmp_path, mutate, status):
+    g = i2.gen_er(50, 100, 1, weighted=False)
+    p = tmp_path / "g.egr"
+    i2.write_eclgraph(g, str(p))
+    raw = np.fromfile(p, np.int32)
+    bad = tmp_path / "bad.egr"
+    np.asarray(mutate(raw), np.int32).tofile(bad)
+    with pytest.raises(i2.I2Error) as e:
+        i2.read_eclgraph(str(bad))
+    assert e.value.status == status
+
+
+def test_out_of_range_neighbour_rejected(tmp_path):
+    g = i2.gen_er(50, 100, 1, weighted=False)
+    nl = g.nlist.copy()
+    nl[3] = g.nodes + 7
+    p = tmp_path / "bad.egr"
+    i2.write_eclgraph(i2.ECLGraph(g.nodes, g.edges, g.nindex, nl, None), str(p))
+    with pytest.raises(i2.I2Error) as e:
+        i2.read_eclgraph(str(p))
+    assert e.value.status == _capi.I2_ERR_FORMAT
+    with pytest.raises(i2.I2Error):
+        i2.read_eclgraph(str(tmp_path / "missing.egr"))
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "i2b200.h").read_text()
+    names = set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(i2_[a-z0-9_]+)\(", header, re.M))
+    assert len(names) >= 35
+    lib = C.CDLL(str(ROOT / "indigo2suite_b200" / "libi2b200.so"))
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_capi.SIGNATURES) <= names | {"i2_gen_rmat_n"}
+
+
+def test_status_and_variant_names():
+    assert i2.lib.i2_status_string(0) == b"ok"
+    assert b"iteration cap" in i2.lib.i2_status_string(_capi.I2_ERR_ITER_CAP)
+    assert [i2.lib.i2_variant_name(k).decode() for k in range(i2.I2_NUM_VARIANTS)] == i2.VARIANTS
+    assert i2.mlp_param_count() == 16 * 2 + 16 * 64 + 64 + 64 * 64 + 64 + 64 * 8 + 8
+
+
+def test_upload_without_device_is_a_status_not_a_crash():
+    if i2.device_count() > 0:
+        pytest.skip("a device is present")
+    g = i2.gen_er(100, 200, 1)
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.upload(g)
+    assert e.value.status == _capi.I2_ERR_NO_DEVICE

@@ -1,0 +1,180 @@
+"""Bit-exact parity of the CUDA engine with the oracle and the golden vectors,
+for every variant, both loop modes, and the per-iteration selectors."""
+import numpy as np
+import pytest
+
+import indigo2suite_b200 as i2
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+FIXED = list(range(i2.I2_NUM_VARIANTS))
+ALL = FIXED + ["heuristic"]
+
+
+def _variants_for(dg):
+    out = []
+    for v in ALL:
+        if v in (4, 5) and not dg.info["symmetric"]:
+            continue
+        out.append(v)
+    return out
+
+
+def test_golden_all_variants_both_loops(gpu, golden):
+    for name, case in golden.items():
+        dg = i2.DeviceGraph.upload(case["graph"])
+        assert dg.info["symmetric"] == 1, name
+        for v in _variants_for(dg):
+            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+                for s in case["sources"]:
+                    d, _ = dg.bfs(s, variant=v, loop=loop)
+                    np.testing.assert_array_equal(d, case["bfs"][s], err_msg=f"{name} bfs {v} {loop} {s}")
+                    d, _ = dg.sssp(s, variant=v, loop=loop)
+                    np.testing.assert_array_equal(d, case["sssp"][s], err_msg=f"{name} sssp {v} {loop} {s}")
+                lab, _ = dg.cc(variant=v, loop=loop)
+                np.testing.assert_array_equal(lab, case["cc"], err_msg=f"{name} cc {v} {loop}")
+        dg.free()
+
+
+def _graphs():
+    return {
+        "er": i2.gen_er(20000, 80000, 3),
+        "rmat14": i2.gen_rmat(14, 16, seed=5),
+        "grid": i2.gen_grid(96, 0.05, 0.002, 7),
+        "rmat16": i2.gen_rmat(16, 16, seed=1),
+    }
+
+
+@pytest.fixture(scope="module")
+def seeded():
+    return _graphs()
+
+
+@pytest.mark.parametrize("name", ["er", "rmat14", "grid", "rmat16"])
+def test_seeded_all_variants_vs_oracle(gpu, seeded, name):
+    g = seeded[name]
+    dg = i2.DeviceGraph.upload(g)
+    src = int(np.argmax(g.degrees()))
+    ref_b, ref_s, ref_c = oracle.bfs(g, src), oracle.sssp(g, src), oracle.cc(g)
+    for v in _variants_for(dg):
+        d, rep = dg.bfs(src, variant=v)
+        np.testing.assert_array_equal(d, ref_b, err_msg=f"bfs {v}")
+        assert rep.reached_vertices == int((ref_b != i2.INF).sum())
+        d, _ = dg.sssp(src, variant=v)
+        np.testing.assert_array_equal(d, ref_s, err_msg=f"sssp {v}")
+        lab, _ = dg.cc(variant=v)
+        np.testing.assert_array_equal(lab, ref_c, err_msg=f"cc {v}")
+    dg.free()
+
+
+def test_heavy_path_and_queue_overflow(gpu, seeded):
+    # A low heavy threshold sends many frontier vertices through the grid-wide
+    # heavy path; a high one keeps hubs in the thread variant (staging overflow).
+    g = seeded["rmat16"]
+    src = int(np.argmax(g.degrees()))
+    ref_b, ref_s, ref_c = oracle.bfs(g, src), oracle.sssp(g, src), oracle.cc(g)
+    dg = i2.DeviceGraph.upload(g)
+    for heavy in (32, 200, 1 << 20):
+        dg.tune(heavy_threshold=heavy)
+        for v in (0, 1, 2, 3, 7, "heuristic"):
+            np.testing.assert_array_equal(dg.bfs(src, variant=v)[0], ref_b, err_msg=f"{heavy} {v}")
+            np.testing.assert_array_equal(dg.sssp(src, variant=v)[0], ref_s, err_msg=f"{heavy} {v}")
+            np.testing.assert_array_equal(dg.cc(variant=v)[0], ref_c, err_msg=f"{heavy} {v}")
+    dg.free()
+
+
+def test_blocks_per_sm_do_not_change_results(gpu, seeded):
+    g = seeded["er"]
+    ref = oracle.sssp(g, 0)
+    dg = i2.DeviceGraph.upload(g)
+    for bps in (1, 2, 8):
+        dg.tune(blocks_per_sm=bps)
+        for v in (0, 2, 4, 6):
+            np.testing.assert_array_equal(dg.sssp(0, variant=v)[0], ref)
+    dg.free()
+
+
+def test_repeated_runs_are_identical_and_independent(gpu, seeded):
+    g = seeded["rmat14"]
+    dg = i2.DeviceGraph.upload(g)
+    ref = oracle.sssp(g, 7)
+    for _ in range(5):
+        np.testing.assert_array_equal(dg.sssp(7, variant="heuristic")[0], ref)
+        dg.bfs(3, variant=1)
+        dg.cc(variant=6)
+    dg.free()
+
+
+def test_multi_source_sources_of_every_vertex_class(gpu, seeded):
+    g = seeded["grid"]
+    dg = i2.DeviceGraph.upload(g)
+    deg = g.degrees()
+    for src in (0, g.nodes - 1, int(np.argmin(deg)), int(np.argmax(deg))):
+        np.testing.assert_array_equal(dg.bfs(src)[0], oracle.bfs(g, src))
+        np.testing.assert_array_equal(dg.sssp(src)[0], oracle.sssp(g, src))
+    dg.free()
+
+
+def test_directed_graph_push_variants_and_pull_refused(gpu):
+    # 0 -> 1 -> 2 -> 3, 4 -> 2 (not symmetric)
+    g = i2.ECLGraph(5, 4, np.array([0, 1, 2, 3, 3, 4], np.int32), np.array([1, 2, 3, 2], np.int32),
+                    np.array([3, 1, 4, 2], np.int32))
+    dg = i2.DeviceGraph.upload(g)
+    assert dg.info["symmetric"] == 0
+    for v in (0, 1, 2, 3, 6, 7, "heuristic"):
+        np.testing.assert_array_equal(dg.bfs(0, variant=v)[0], oracle.bfs(g, 0))
+        np.testing.assert_array_equal(dg.sssp(4, variant=v)[0], oracle.sssp(g, 4))
+        np.testing.assert_array_equal(dg.cc(variant=v)[0], oracle.cc(g))
+    for v in (4, 5):
+        with pytest.raises(i2.I2Error) as e:
+            dg.bfs(0, variant=v)
+        assert e.value.status == i2._capi.I2_ERR_UNSUPPORTED
+    dg.free()
+
+
+def test_single_vertex_and_edgeless_graphs(gpu):
+    g1 = i2.ECLGraph(1, 0, np.array([0, 0], np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    g2 = i2.ECLGraph(70, 0, np.zeros(71, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    for g in (g1, g2):
+        dg = i2.DeviceGraph.upload(g)
+        for v in ALL:
+            np.testing.assert_array_equal(dg.bfs(0, variant=v)[0], oracle.bfs(g, 0))
+            np.testing.assert_array_equal(dg.sssp(0, variant=v)[0], oracle.sssp(g, 0))
+            np.testing.assert_array_equal(dg.cc(variant=v)[0], np.arange(g.nodes))
+        dg.free()
+
+
+def test_records_and_report(gpu, seeded):
+    g = seeded["rmat14"]
+    dg = i2.DeviceGraph.upload(g)
+    src = int(np.argmax(g.degrees()))
+    d, rep = dg.bfs(src, variant="heuristic", record=True)
+    recs = dg.records()
+    assert len(recs) == rep.iterations > 0
+    assert sum(rep.variant_hist) == rep.iterations
+    assert recs[0]["size"] + recs[0]["hsize"] == 1
+    assert all(r["t_ns"] > 0 for r in recs)
+    assert rep.seconds > 0 and 0 < rep.relax_seconds <= rep.seconds * 1.5
+    reached = d != i2.INF
+    assert rep.reached_vertices == reached.sum()
+    assert rep.reached_edges == g.degrees()[reached].sum()
+    dg.free()
+
+
+def test_reference_interface_mirror(gpu, golden):
+    case = golden["rmat_s10_ef16_s3"]
+    g = case["graph"]
+    dg = i2.DeviceGraph.upload(g)
+    out = np.empty(g.nodes, np.int32)
+    for fn in (i2.GPUbfs_vertex, i2.GPUbfs_edge):
+        t = fn(0, dg, out)
+        assert t > 0
+        np.testing.assert_array_equal(out, case["bfs"][0])
+    for fn in (i2.GPUsssp_vertex, i2.GPUsssp_edge):
+        fn(0, dg, out)
+        np.testing.assert_array_equal(out, case["sssp"][0])
+    for fn in (i2.GPUcc_vertex, i2.GPUcc_edge):
+        fn(dg, out)
+        np.testing.assert_array_equal(out, case["cc"])
+    dg.free()
