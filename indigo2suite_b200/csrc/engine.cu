@@ -1061,10 +1061,46 @@ int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
   return I2_OK;
 }
 
+// True when [p, p + bytes) lies inside one device (or managed) allocation of
+// the current context. Host pointers, pinned or not, are refused: a kernel
+// given one would fault or read the wrong memory.
+typedef int (*MemGetAddressRangeFn)(unsigned long long*, size_t*, unsigned long long);
+
+static bool device_range_ok(const void* p, size_t bytes) {
+  if (bytes == 0) return true;
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+  static MemGetAddressRangeFn range_fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range_fn = (MemGetAddressRangeFn)fn;
+    cudaGetLastError();
+  }
+  if (!range_fn) return true;  // type check only
+  unsigned long long base = 0;
+  size_t size = 0;
+  if (range_fn(&base, &size, (unsigned long long)(uintptr_t)p) != 0) return false;
+  return (unsigned long long)(uintptr_t)p + bytes <= base + size;
+}
+
 int i2_graph_wrap_device(const i2_eclgraph* d, i2_graph** out) {
   if (!d || !out || d->nodes < 1 || d->edges < 0 || !d->nindex || (d->edges > 0 && !d->nlist)) return I2_ERR_ARG;
   *out = nullptr;
   if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
+  if (!device_range_ok(d->nindex, sizeof(int) * ((size_t)d->nodes + 1)) ||
+      !device_range_ok(d->nlist, sizeof(int) * (size_t)d->edges) ||
+      (d->eweight && !device_range_ok(d->eweight, sizeof(int) * (size_t)d->edges)))
+    return I2_ERR_ARG;
   i2_graph* g = new i2_graph();
   g->owns = false;
   g->d_nindex = d->nindex;

@@ -11,5 +11,5 @@ static const int ThreadsPerBlock = 512;
 static double GPUbfs_edge(const int src, const ECLgraph& g, basic_t* const dist, const int* const sp)
 {
   (void)sp;  // the engine builds its own starting-point array on the device when needed
-  return i2shim_run(I2_BFS, src, g.nodes, g.edges, g.nindex, g.nlist, g.eweight, dist, I2_VP_CTA);
+  return i2shim_run(I2_BFS, src, g.nodes, g.edges, g.nindex, g.nlist, nullptr, dist, I2_VP_CTA);
 }

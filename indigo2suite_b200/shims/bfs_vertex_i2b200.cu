@@ -10,5 +10,5 @@ static const int ThreadsPerBlock = 512;
 
 static double GPUbfs_vertex(const int src, const ECLgraph& g, basic_t* const dist)
 {
-  return i2shim_run(I2_BFS, src, g.nodes, g.edges, g.nindex, g.nlist, g.eweight, dist, I2_AUTO_HEURISTIC);
+  return i2shim_run(I2_BFS, src, g.nodes, g.edges, g.nindex, g.nlist, nullptr, dist, I2_AUTO_HEURISTIC);
 }

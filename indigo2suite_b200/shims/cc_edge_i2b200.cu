@@ -11,5 +11,5 @@ static const int ThreadsPerBlock = 512;
 static double GPUcc_edge(const ECLgraph& g, basic_t* const label, const int* const sp)
 {
   (void)sp;  // the engine builds its own starting-point array on the device when needed
-  return i2shim_run(I2_CC, 0, g.nodes, g.edges, g.nindex, g.nlist, g.eweight, label, I2_EDGE_TOPO);
+  return i2shim_run(I2_CC, 0, g.nodes, g.edges, g.nindex, g.nlist, nullptr, label, I2_EDGE_TOPO);
 }

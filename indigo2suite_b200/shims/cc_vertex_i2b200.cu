@@ -10,5 +10,5 @@ static const int ThreadsPerBlock = 512;
 
 static double GPUcc_vertex(const ECLgraph& g, basic_t* const label)
 {
-  return i2shim_run(I2_CC, 0, g.nodes, g.edges, g.nindex, g.nlist, g.eweight, label, I2_AUTO_HEURISTIC);
+  return i2shim_run(I2_CC, 0, g.nodes, g.edges, g.nindex, g.nlist, nullptr, label, I2_AUTO_HEURISTIC);
 }

@@ -7,7 +7,10 @@
 // implements the harness's GPU<alg>_<kind>() entry point on top of the C ABI
 // of libi2b200 (include/i2b200.h). The harness passes the graph with device
 // pointers (its d_g) and a host result array; the shim wraps the device arrays
-// without copying them and returns the engine's device time in seconds.
+// without copying them and returns the engine's device time in seconds. Only
+// the SSSP harnesses upload the weights (include/sssp_vertex_cuda.h:122-125);
+// in the BFS and CC harnesses d_g.eweight is still the host array from the file
+// reader, so those shims pass no weights.
 //
 // $I2_VARIANT selects the style: a variant name (vp_thread, vp_warp, vp_cta,
 // vp_block, pull_frontier, pull_topo, edge_topo, push_topo), "heuristic"

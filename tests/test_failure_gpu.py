@@ -71,3 +71,21 @@ def test_malformed_device_graph_rejected_before_any_traversal(gpu):
         i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
     assert e.value.status == _capi.I2_ERR_FORMAT
     torch.cuda.synchronize()
+
+
+def test_wrap_refuses_host_pointers(gpu):
+    # The reference's BFS/CC harnesses keep d_g.eweight on the host; a host
+    # pointer handed over as device memory must be refused, not dereferenced.
+    g = i2.gen_er(64, 128, 4)
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.wrap_device(g.nodes, g.edges, g.nindex.ctypes.data, g.nlist.ctypes.data)
+    assert e.value.status == _capi.I2_ERR_ARG
+    import torch
+
+    ni = torch.tensor(g.nindex, dtype=torch.int32, device="cuda")
+    nl = torch.tensor(g.nlist, dtype=torch.int32, device="cuda")
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), g.eweight.ctypes.data)
+    assert e.value.status == _capi.I2_ERR_ARG
+    ok = i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
+    ok.free()
