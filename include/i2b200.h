@@ -155,13 +155,17 @@ int i2_graph_wrap_device(const i2_eclgraph* dev, i2_graph** out);
 /* Generate an RMAT graph directly on the device (identical CSR to i2_gen_rmat). */
 int i2_graph_generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
                            int weighted, i2_graph** out);
+int i2_graph_size(const i2_graph* g, int* nodes, int* edges);
+/* Statistics of the graph; the first call also checks symmetry (one pass over the CSR). */
 int i2_graph_info_get(const i2_graph* g, i2_graph_info* out);
 /* Copy the device CSR back to a host graph allocated by the callee. */
 int i2_graph_download(const i2_graph* g, i2_eclgraph* out);
 /* Launch tuning of a graph: degree threshold from which a frontier vertex is
-   split across the whole grid (heavy path), and resident blocks per SM of the
-   relax kernels. 0 keeps the current value. Results do not depend on either. */
-int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm);
+   split across the whole grid (heavy path; 0 keeps it), cap on resident blocks
+   per SM of the relax kernels (0 keeps it), and the preferred shared-memory
+   carveout in percent (-1: driver default; applies process-wide). Results do
+   not depend on any of them. */
+int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_carveout);
 /* Give the graph the reference's synthetic weights when it has none (on the device). */
 int i2_graph_synth_weights(i2_graph* g);
 int i2_graph_free(i2_graph* g);

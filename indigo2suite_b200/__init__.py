@@ -191,10 +191,16 @@ class DeviceGraph:
     def __init__(self, handle: C.c_void_p, host: ECLGraph | None = None):
         self._h = handle
         self.host = host
+        n, e = C.c_int(), C.c_int()
+        _check(lib.i2_graph_size(self._h, C.byref(n), C.byref(e)), "graph size")
+        self.nodes, self.edges = n.value, e.value
+
+    @property
+    def info(self) -> dict:
+        """Graph statistics (the first query also checks symmetry on the device)."""
         info = capi.GraphInfo()
         _check(lib.i2_graph_info_get(self._h, C.byref(info)), "graph info")
-        self.nodes, self.edges = info.nodes, info.edges
-        self.info = {k: getattr(info, k) for k, _ in capi.GraphInfo._fields_}
+        return {k: getattr(info, k) for k, _ in capi.GraphInfo._fields_}
 
     @classmethod
     def upload(cls, g: ECLGraph) -> "DeviceGraph":
@@ -227,17 +233,11 @@ class DeviceGraph:
         _check(lib.i2_graph_download(self._h, C.byref(cg)), "graph download")
         return ECLGraph._from_c(cg)
 
-    def tune(self, heavy_threshold: int = 0, blocks_per_sm: int = 0) -> None:
-        _check(lib.i2_graph_tune(self._h, heavy_threshold, blocks_per_sm), "tune")
-        info = capi.GraphInfo()
-        lib.i2_graph_info_get(self._h, C.byref(info))
-        self.info = {k: getattr(info, k) for k, _ in capi.GraphInfo._fields_}
+    def tune(self, heavy_threshold: int = 0, blocks_per_sm: int = 0, smem_carveout: int = -1) -> None:
+        _check(lib.i2_graph_tune(self._h, heavy_threshold, blocks_per_sm, smem_carveout), "tune")
 
     def synth_weights(self) -> None:
         _check(lib.i2_graph_synth_weights(self._h), "synth weights")
-        info = capi.GraphInfo()
-        lib.i2_graph_info_get(self._h, C.byref(info))
-        self.info = {k: getattr(info, k) for k, _ in capi.GraphInfo._fields_}
 
     def free(self) -> None:
         if self._h:

@@ -86,10 +86,11 @@ SIGNATURES = {
     "i2_graph_wrap_device": (_I, [_PG, C.POINTER(_P)]),
     "i2_graph_generate_rmat": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I,
                                     C.POINTER(_P)]),
+    "i2_graph_size": (_I, [_P, _PI, _PI]),
     "i2_graph_info_get": (_I, [_P, C.POINTER(GraphInfo)]),
     "i2_graph_download": (_I, [_P, _PG]),
     "i2_graph_synth_weights": (_I, [_P]),
-    "i2_graph_tune": (_I, [_P, _I, _I]),
+    "i2_graph_tune": (_I, [_P, _I, _I, _I]),
     "i2_gen_rmat_n": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I, _PG]),
     "i2_graph_free": (_I, [_P]),
     "i2_bfs": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),

@@ -10,9 +10,13 @@
 // Frontier contract shared by every variant (so a selector may switch variant
 // at any iteration without changing the result):
 //   at the start of iteration i, F_i is stored in slot s = i % 3 as
-//     wl[s][0..size)    light vertices (degree < heavy threshold),
-//     hwl[s][0..hsize)  heavy vertices,
-//     bm[s]             a bitmap with exactly the bits of F_i set;
+//     wl[s][0..size)     its vertices (those of degree >= 1),
+//     woff[s][0..size)   the exclusive prefix sum of their degrees, so that
+//                        the frontier's edges form one index space [0, edges),
+//     hwl[s][0..hsize)   the subset of degree >= the heavy threshold, with
+//     htoff[s][0..hsize) the exclusive prefix of their tile counts,
+//     bm[s]              a bitmap with the bits of F_i set (vertices of
+//                        degree 0 are never kept: they have nothing to relax);
 //   every vertex outside F_i has already relaxed all of its out-edges against
 //   the current dist[]. Iteration i propagates at least F_i and builds F_{i+1}
 //   in slot (i+1) % 3 from every vertex whose value it lowered. It also clears
@@ -71,15 +75,20 @@ struct GStats {
   float degcv;      // coefficient of variation of the degree distribution
 };
 
-// Statistics of one frontier buffer, accumulated while it is built.
+// Statistics of one frontier buffer, accumulated while it is built. Entries
+// and edges share one 64-bit word (entries << 32 | edges) so that a single
+// atomicAdd hands out consistent positions in wl[] and offsets in woff[]; a
+// frontier holds each vertex at most once, so edges <= E < 2^31 never carries
+// into the entry count. The heavy list pairs entries with tiles the same way.
 struct Slot {
-  int size;                 // light entries
-  int hsize;                // heavy entries
-  unsigned long long edges; // sum of degrees over all entries
+  unsigned long long packed;  // entries << 32 | edges
+  unsigned long long hpacked; // heavy entries << 32 | heavy tiles
   int maxdeg;
-  int mindist;              // smallest value pushed into this frontier
-  int pad[2];
+  int mindist;                // smallest value pushed into this frontier
 };
+
+__host__ __device__ __forceinline__ int slot_size(unsigned long long p) { return (int)(p >> 32); }
+__host__ __device__ __forceinline__ unsigned slot_edges(unsigned long long p) { return (unsigned)(p & 0xffffffffu); }
 
 struct Ctl {
   Slot slot[3];
@@ -88,7 +97,9 @@ struct Ctl {
   int status;               // error bits, see kStatus*
   int variant;              // variant to run at the next launch
   unsigned done;            // blocks finished in the current launch
-  int chunk;                // dynamic chunk counter of the current launch
+  int chunk;                // dynamic work counter of the current launch
+  int htile;                // dynamic heavy-tile counter of the current launch
+  int pad0;
   unsigned long long tstart;// earliest block start of the current launch (globaltimer ns)
   long long visited;        // vertices reached so far
   int hist[kMaxVariants];   // launches per variant
@@ -128,7 +139,9 @@ struct Ctx {
   GStats gs;
   int* dist;
   int* wl[3];
+  unsigned* woff[3];
   int* hwl[3];
+  unsigned* htoff[3];
   unsigned* bm[3];
   Ctl* ctl;
   IterRec* recs;

@@ -32,16 +32,16 @@ static_assert((int)kNumVariants == (int)I2_NUM_VARIANTS, "variant count");
 // ---------------------------------------------------------------------------
 // Selection of the next variant.
 
-__device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, int hsize,
-                              unsigned long long edges) {
-  const float fs = (float)size + (float)hsize;
+// Fixed frontier-size rule: bottom-up pull for BFS levels whose frontier
+// carries more than 1/16 of the edges (direction-optimising BFS), otherwise the
+// edge-balanced push, which measured fastest of the push styles on every
+// family tried.
+__device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, unsigned long long edges) {
+  (void)size;
   const float fe = (float)edges;
   const float E = (float)gs.edges;
   auto ok = [&](int v) { return (allowed >> v) & 1; };
   if (algo == kBFS && ok(kPullFrontier) && fe > E * (1.f / 16.f)) return kPullFrontier;
-  if (ok(kEdgeTopo) && fe > E * 0.5f) return kEdgeTopo;
-  const float mean = fe / fmaxf(1.f, fs);
-  if (mean >= 64.f && ok(kVPWarp)) return kVPWarp;
   return ok(kVPCta) ? kVPCta : kVPThread;
 }
 
@@ -53,7 +53,8 @@ __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
   Ctl* ctl = c.ctl;
   if (threadIdx.x == 0) {
     volatile Slot* sl = &ctl->slot[nxt];
-    frontier_features(c.gs, ctl->algo, next_iter, sl->size, sl->hsize, sl->edges, sl->maxdeg,
+    const unsigned long long p = sl->packed;
+    frontier_features(c.gs, ctl->algo, next_iter, slot_size(p), slot_size(sl->hpacked), slot_edges(p), sl->maxdeg,
                       *(volatile long long*)&ctl->visited, x);
     for (int k = 0; k < kFeatures; ++k) ctl->feat[k] = x[k];
   }
@@ -64,7 +65,8 @@ __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
     int v = ctl->fixed_variant;
     if (mode == 1 || (mode == 2 && !c.mlp)) {
       volatile Slot* sl = &ctl->slot[nxt];
-      v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, sl->size, sl->hsize, sl->edges);
+      const unsigned long long p = sl->packed;
+      v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, slot_size(p), slot_edges(p));
     } else if (mode == 2) {
       float best = 3.0e38f;
       v = -1;
@@ -96,9 +98,9 @@ __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old)
       IterRec& r = c.recs[i];
       r.iter = i;
       r.variant = ctl->variant;
-      r.size = sc->size;
-      r.hsize = sc->hsize;
-      r.edges = sc->edges;
+      r.size = slot_size(sc->packed);
+      r.hsize = slot_size(sc->hpacked);
+      r.edges = slot_edges(sc->packed);
       r.maxdeg = sc->maxdeg;
       r.mindist = sc->mindist;
       r.visited = *(volatile long long*)&ctl->visited;
@@ -106,17 +108,17 @@ __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old)
       for (int k = 0; k < kFeatures; ++k) r.feat[k] = ctl->feat[k];
     }
     Slot& so = ctl->slot[old];
-    so.size = 0;
-    so.hsize = 0;
-    so.edges = 0;
+    so.packed = 0;
+    so.hpacked = 0;
     so.maxdeg = 0;
     so.mindist = kInf;
     ctl->done = 0;
     ctl->chunk = 0;
+    ctl->htile = 0;
     ctl->tstart = ~0ull;
     ctl->iter = i + 1;
     volatile Slot* sn = &ctl->slot[nxt];
-    const long long n = (long long)sn->size + sn->hsize;
+    const long long n = slot_size(sn->packed);
     int cond = n > 0;
     if (cond && i + 1 >= ctl->iter_cap) {
       ctl->status |= kStatusIterCap;
@@ -136,6 +138,8 @@ template <int ALG>
 __global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
   __shared__ Stage s;
   stage_init(s);
+  Acc a;
+  acc_init(a);
   __syncthreads();
   const int V = c.g.nodes;
   for (long long base = (long long)blockIdx.x * kBlock; base < V; base += (long long)gridDim.x * kBlock) {
@@ -143,23 +147,25 @@ __global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
     const bool in = v < V;
     if (in) c.dist[v] = (ALG == kCC) ? v : kInf;
     if (ALG == kCC) {
-      const unsigned word = __ballot_sync(0xffffffffu, in);
+      const int deg = in ? c.g.nindex[v + 1] - c.g.nindex[v] : 0;
+      const bool put = in && deg > 0;  // vertices without edges are already final
+      const unsigned word = __ballot_sync(0xffffffffu, put);
       if ((threadIdx.x & 31) == 0 && word) c.bm[0][v >> 5] = word;
-      if (in) {
-        atomicMin(&s.mindist, v);
-        stage_vertex(c, s, 0, v);
+      if (put) {
+        a.mindist = min(a.mindist, v);
+        stage_entry(c, s, a, 0, v, deg);
       }
       stage_flush(c, s, 0);
     }
   }
   if (ALG == kCC) {
     stage_flush(c, s, 0);
-    __syncthreads();
+    acc_reduce(a, s);
     if (threadIdx.x == 0) {
+      const Acc& r = s.red[0];
       Slot& sl = c.ctl->slot[0];
-      if (s.edges) atomicAdd(&sl.edges, s.edges);
-      if (s.maxdeg) atomicMax(&sl.maxdeg, s.maxdeg);
-      if (s.mindist != kInf) atomicMin(&sl.mindist, s.mindist);
+      if (r.maxdeg) atomicMax(&sl.maxdeg, r.maxdeg);
+      if (r.mindist != kInf) atomicMin(&sl.mindist, r.mindist);
     }
   }
 }
@@ -172,17 +178,27 @@ __global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
     const int ns = c.srcs ? ctl->nsrc : 1;
     for (int j = threadIdx.x; j < ns; j += blockDim.x) {
       const int v = c.srcs ? c.srcs[j] : ctl->src;
+      const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
       const unsigned bit = 1u << (v & 31);
       if (atomicOr(&c.bm[0][v >> 5], bit) & bit) continue;
       c.dist[v] = 0;
-      const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
-      Slot& sl = ctl->slot[0];
-      atomicAdd(&sl.edges, (unsigned long long)deg);
-      atomicMax(&sl.maxdeg, deg);
-      atomicMin(&sl.mindist, 0);
       atomicAdd((unsigned long long*)&ctl->visited, 1ull);
-      if (deg >= c.heavy) c.hwl[0][atomicAdd(&sl.hsize, 1)] = v;
-      else c.wl[0][atomicAdd(&sl.size, 1)] = v;
+      Slot& sl = ctl->slot[0];
+      atomicMin(&sl.mindist, 0);
+      if (deg == 0) {
+        atomicAnd(&c.bm[0][v >> 5], ~bit);  // nothing to propagate
+        continue;
+      }
+      atomicMax(&sl.maxdeg, deg);
+      const unsigned long long b = atomicAdd(&sl.packed, (1ull << 32) | (unsigned)deg);
+      c.wl[0][slot_size(b)] = v;
+      c.woff[0][slot_size(b)] = slot_edges(b);
+      if (deg >= c.heavy) {
+        const int t = heavy_tiles(deg);
+        const unsigned long long hb = atomicAdd(&sl.hpacked, (1ull << 32) | (unsigned)t);
+        c.hwl[0][slot_size(hb)] = v;
+        c.htoff[0][slot_size(hb)] = slot_edges(hb);
+      }
     }
   } else if (threadIdx.x == 0) {
     ctl->visited = c.g.nodes;
@@ -249,7 +265,6 @@ __global__ void k_degree_stats(DGraph g, int heavy, DevStats* st) {
     mx = max(mx, d);
     nh += d >= heavy;
     s2 += (double)d * d;
-    for (int k = b + 1; k < e && !uns; ++k) uns |= g.nlist[k] <= g.nlist[k - 1];
   }
   int wmin = INT_MAX;
   if (g.eweight)
@@ -261,32 +276,45 @@ __global__ void k_degree_stats(DGraph g, int heavy, DevStats* st) {
   atomicAdd(&st->sumsq, s2);
 }
 
-// For every entry (u, v, w): is (v, u, w) present? Binary search (adjacency sorted).
-__global__ void k_symmetry(DGraph g, DevStats* st) {
+// Adjacency lists strictly increasing (sorted, no duplicates)? One thread per
+// CSR entry, using the starting-point array for the entry's row.
+__global__ void k_sorted(DGraph g, const int* __restrict__ sp, DevStats* st) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int uns = 0;
+  for (long long e = 1 + tid; e < g.edges; e += stride)
+    uns |= (sp[e] == sp[e - 1]) && (g.nlist[e] <= g.nlist[e - 1]);
+  if (uns) atomicOr(&st->unsorted, 1);
+}
+
+// For every entry (u, v, w): is (v, u, w) present? One thread per entry,
+// binary search in v's sorted adjacency.
+__global__ void k_symmetry(DGraph g, const int* __restrict__ sp, DevStats* st) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   int asym = 0;
-  for (long long v = tid; v < g.nodes && !asym; v += stride) {
-    for (int k = g.nindex[v]; k < g.nindex[v + 1]; ++k) {
-      const int u = g.nlist[k];
-      int lo = g.nindex[u], hi = g.nindex[u + 1] - 1, pos = -1;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const int x = g.nlist[mid];
-        if (x == (int)v) { pos = mid; break; }
-        if (x < (int)v) lo = mid + 1; else hi = mid - 1;
-      }
-      if (pos < 0 || (g.eweight && g.eweight[pos] != g.eweight[k])) { asym = 1; break; }
+  for (long long k = tid; k < g.edges && !asym; k += stride) {
+    const int u = sp[k];
+    const int v = g.nlist[k];
+    int lo = g.nindex[v], hi = g.nindex[v + 1] - 1, pos = -1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const int x = g.nlist[mid];
+      if (x == u) { pos = mid; break; }
+      if (x < u) lo = mid + 1; else hi = mid - 1;
     }
+    if (pos < 0 || (g.eweight && g.eweight[pos] != g.eweight[k])) asym = 1;
   }
   if (asym) atomicOr(&st->asym, 1);
 }
 
+// sp[k] = row of CSR entry k; one warp per vertex, coalesced stores.
 __global__ void k_build_sp(DGraph g, int* sp) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long v = tid; v < g.nodes; v += stride)
-    for (int k = g.nindex[v]; k < g.nindex[v + 1]; ++k) sp[k] = (int)v;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (long long v = warp; v < g.nodes; v += nwarps)
+    for (int k = g.nindex[v] + lane; k < g.nindex[v + 1]; k += 32) sp[k] = (int)v;
 }
 
 // Reference synthetic weights (include/sssp_vertex_cuda.h:127-137) on the device.
@@ -331,7 +359,7 @@ static KernelFn relax_fn(int v) {
   switch (v) {
     case kVPThread: return relax_push<ALG, kVPThread>;
     case kVPWarp: return relax_push<ALG, kVPWarp>;
-    case kVPCta: return relax_push<ALG, kVPCta>;
+    case kVPCta: return relax_edge_balanced<ALG>;
     case kVPBlock: return relax_push<ALG, kVPBlock>;
     case kPullFrontier: return relax_pull<ALG, true>;
     case kPullTopo: return relax_pull<ALG, false>;
@@ -388,7 +416,13 @@ static int sm_count() {
   return n;
 }
 
+// Preferred shared-memory carveout (percent of the unified L1/shared storage)
+// for the relax kernels; -1 leaves the choice to the driver. A large carveout
+// costs L1 capacity, which the adjacency reads use.
+static int g_carveout = -1;
+
 int grid_for(KernelFn fn, int max_per_sm) {
+  cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout, g_carveout);
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, kBlock, 0);
   per = std::max(1, std::min(per, max_per_sm));
@@ -452,12 +486,14 @@ struct i2_graph {
   bool owns_weights = false;
   int* d_sp = nullptr;
   int heavy = 4096;
-  int blocks_per_sm = 4;
+  int blocks_per_sm = 8;  // cap; the occupancy of each kernel decides below it
   // workspace
   bool ws_ready = false;
   int* dist = nullptr;
   int* wl[3] = {nullptr, nullptr, nullptr};
+  unsigned* woff[3] = {nullptr, nullptr, nullptr};
   int* hwl[3] = {nullptr, nullptr, nullptr};
+  unsigned* htoff[3] = {nullptr, nullptr, nullptr};
   unsigned* bm[3] = {nullptr, nullptr, nullptr};
   int bm_words = 0;
   Ctl* ctl = nullptr;
@@ -493,7 +529,9 @@ static void free_graph_state(i2_graph* g) {
   cudaFree(g->dist);
   for (int k = 0; k < 3; ++k) {
     cudaFree(g->wl[k]);
+    cudaFree(g->woff[k]);
     cudaFree(g->hwl[k]);
+    cudaFree(g->htoff[k]);
   }
   cudaFree(g->bm[0]);
   cudaFree(g->ctl);
@@ -528,13 +566,6 @@ static int compute_stats(i2_graph* g) {
   k_degree_stats<<<grid, 256, 0, g->stream>>>(g->g, g->heavy, st);
   cudaStreamSynchronize(g->stream);
   cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost);
-  if (!h.unsorted) {
-    k_symmetry<<<grid, 256, 0, g->stream>>>(g->g, st);
-    cudaStreamSynchronize(g->stream);
-    int asym = 0;
-    cudaMemcpy(&asym, &st->asym, sizeof(int), cudaMemcpyDeviceToHost);
-    h.asym = asym;
-  }
   cudaError_t e = cudaGetLastError();
   cudaFree(st);
   if (e != cudaSuccess) return cuda_status(e);
@@ -544,7 +575,7 @@ static int compute_stats(i2_graph* g) {
   s.maxdeg = h.maxdeg;
   s.nheavy = h.nheavy;
   s.wmin = g->g.eweight ? (h.wmin == INT_MAX ? 1 : h.wmin) : 1;
-  s.symmetric = (!h.unsorted && !h.asym) ? 1 : 0;
+  s.symmetric = -1;  // decided on first need (ensure_symmetry)
   const double mean = (double)g->g.edges / (double)g->g.nodes;
   const double var = std::max(0.0, h.sumsq / (double)g->g.nodes - mean * mean);
   s.avgdeg = (float)mean;
@@ -571,7 +602,9 @@ static int ensure_workspace(i2_graph* g) {
   I2_CK(cudaMalloc(&g->dist, sizeof(int) * V));
   for (int k = 0; k < 3; ++k) {
     I2_CK(cudaMalloc(&g->wl[k], sizeof(int) * V));
+    I2_CK(cudaMalloc(&g->woff[k], sizeof(unsigned) * V));
     I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+    I2_CK(cudaMalloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
   }
   unsigned* bm = nullptr;
   I2_CK(cudaMalloc(&bm, sizeof(unsigned) * 3ull * g->bm_words));
@@ -593,10 +626,37 @@ static int ensure_sp(i2_graph* g) {
   return I2_OK;
 }
 
+// Pull variants read a vertex's out-list as its in-list, so they need every
+// (u, v, w) to have a (v, u, w) partner. Checked once, on first need.
+static int ensure_symmetry(i2_graph* g) {
+  if (g->gs.symmetric >= 0) return I2_OK;
+  int st = ensure_sp(g);
+  if (st) return st;
+  DevStats* d = nullptr;
+  I2_CK(cudaMalloc(&d, sizeof(DevStats)));
+  DevStats h{};
+  cudaMemcpy(d, &h, sizeof(h), cudaMemcpyHostToDevice);
+  const int grid = 8 * sm_count();
+  k_sorted<<<grid, 256, 0, g->stream>>>(g->g, g->d_sp, d);
+  cudaStreamSynchronize(g->stream);
+  cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  if (!h.unsorted) {
+    k_symmetry<<<grid, 256, 0, g->stream>>>(g->g, g->d_sp, d);
+    cudaStreamSynchronize(g->stream);
+    cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_status(e);
+  g->gs.symmetric = (!h.unsorted && !h.asym) ? 1 : 0;
+  drop_execs(g);  // graphs bake the statistics into their arguments
+  return I2_OK;
+}
+
 static int allowed_mask(const i2_graph* g) {
   int m = 0;
   for (int v = 0; v < kNumVariants; ++v) m |= 1 << v;
-  if (!g->gs.symmetric) m &= ~((1 << kPullFrontier) | (1 << kPullTopo));
+  if (g->gs.symmetric != 1) m &= ~((1 << kPullFrontier) | (1 << kPullTopo));
   if (!g->d_sp) m &= ~(1 << kEdgeTopo);
   return m;
 }
@@ -608,7 +668,9 @@ static Ctx make_ctx(const i2_graph* g) {
   c.dist = g->dist;
   for (int k = 0; k < 3; ++k) {
     c.wl[k] = g->wl[k];
+    c.woff[k] = g->woff[k];
     c.hwl[k] = g->hwl[k];
+    c.htoff[k] = g->htoff[k];
     c.bm[k] = g->bm[k];
   }
   c.ctl = g->ctl;
@@ -773,7 +835,7 @@ static int run_host_loop(i2_graph* g, cudaStream_t s, int algo, bool multi, doub
     I2_CK(cudaMemcpyAsync(h, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     I2_CK(cudaStreamSynchronize(s));
     const int cur = h->iter % 3;
-    const long long n = (long long)h->slot[cur].size + h->slot[cur].hsize;
+    const long long n = slot_size(h->slot[cur].packed);
     if (n == 0 || (h->status & kStatusIterCap)) break;
     KernelFn fn = relax_kernel(algo, h->variant);
     I2_CK(cudaEventRecord(g->ev2, s));
@@ -833,6 +895,10 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   else if (variant < 0 || variant >= kNumVariants) return I2_ERR_ARG;
   if (mode != 0 || variant == kEdgeTopo) {
     st = ensure_sp(g);
+    if (st) return st;
+  }
+  if (mode != 0 || variant == kPullFrontier || variant == kPullTopo) {
+    st = ensure_symmetry(g);
     if (st) return st;
   }
   if (mode == 0 && !((allowed_mask(g) >> variant) & 1)) return I2_ERR_UNSUPPORTED;
@@ -912,7 +978,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
   I2_CK(cudaSetDevice(g->device));
   int st = ensure_workspace(g);
   if (st) return st;
-  st = ensure_sp(g);
+  st = ensure_symmetry(g);
   if (st) return st;
   const long long V = g->g.nodes;
   if (!g->snap_dist) {
@@ -935,7 +1001,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
     I2_CK(cudaStreamSynchronize(s));
     snap = *g->h_ctl;
     const int cur = snap.iter % 3;
-    if ((long long)snap.slot[cur].size + snap.slot[cur].hsize == 0) break;
+    if (slot_size(snap.slot[cur].packed) == 0) break;
     I2_CK(cudaMemcpyAsync(g->snap_dist, g->dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
     I2_CK(cudaMemcpyAsync(g->snap_bm, g->bm[0], sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
     for (int v = 0; v < kNumVariants; ++v) {
@@ -1136,8 +1202,20 @@ int i2_graph_wrap_device(const i2_eclgraph* d, i2_graph** out) {
   return I2_OK;
 }
 
+int i2_graph_size(const i2_graph* g, int* nodes, int* edges) {
+  if (!g || !nodes || !edges) return I2_ERR_ARG;
+  *nodes = g->g.nodes;
+  *edges = g->g.edges;
+  return I2_OK;
+}
+
 int i2_graph_info_get(const i2_graph* g, i2_graph_info* out) {
   if (!g || !out) return I2_ERR_ARG;
+  if (g->gs.symmetric < 0) {
+    cudaSetDevice(g->device);
+    const int st = ensure_symmetry(const_cast<i2_graph*>(g));
+    if (st) return st;
+  }
   out->nodes = g->gs.nodes;
   out->edges = g->gs.edges;
   out->maxdeg = g->gs.maxdeg;
@@ -1166,8 +1244,10 @@ int i2_graph_download(const i2_graph* g, i2_eclgraph* out) {
   return I2_OK;
 }
 
-int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm) {
+int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_carveout) {
   if (!g || heavy_threshold < 0 || blocks_per_sm < 0 || blocks_per_sm > 32) return I2_ERR_ARG;
+  if (smem_carveout < -1 || smem_carveout > 100) return I2_ERR_ARG;
+  g_carveout = smem_carveout;
   I2_CK(cudaSetDevice(g->device));
   if (g->stream) I2_CK(cudaStreamSynchronize(g->stream));
   drop_execs(g);
@@ -1177,12 +1257,17 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm) {
     // the heavy lists are sized by the number of heavy vertices
     for (int k = 0; k < 3; ++k) {
       cudaFree(g->hwl[k]);
+      cudaFree(g->htoff[k]);
       g->hwl[k] = nullptr;
+      g->htoff[k] = nullptr;
     }
     int st = compute_stats(g);
     if (st) return st;
     if (g->ws_ready)
-      for (int k = 0; k < 3; ++k) I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+      for (int k = 0; k < 3; ++k) {
+        I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+        I2_CK(cudaMalloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
+      }
   }
   return I2_OK;
 }
@@ -1261,7 +1346,7 @@ int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_recor
   if (algo != I2_CC && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
   if (algo == I2_SSSP && !g->g.eweight) return I2_ERR_ARG;
   if (follow >= 0) {
-    int st = ensure_sp(g);
+    int st = ensure_symmetry(g);
     if (st) return st;
     if (!((allowed_mask(g) >> follow) & 1)) return I2_ERR_UNSUPPORTED;
   }

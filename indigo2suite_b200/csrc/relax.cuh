@@ -6,18 +6,27 @@
 //   kVPThread  ~ *_V_Data_Push_*_Thread_*   (e.g. BFS ..._Atomic_Thread_..._NonDup.cu)
 //   kVPWarp    ~ *_V_Data_Push_*_Warp_*     (BFS_CUDA_V_Data_Push_..._Warp_..._NonDup.cu:62-84)
 //   kVPBlock   ~ *_V_Data_Push_*_Block_*    (BFS_CUDA_V_Data_Push_..._Block_..._Dup.cu:62-83)
-//   kVPCta     ~ *_E_Data_Push_*            (SSSP_CUDA_E_Data_Push_..._NonDup.cu:63-82): one thread per edge
+//   kVPCta     ~ *_E_Data_Push_*            (SSSP_CUDA_E_Data_Push_..._NonDup.cu:63-82): one thread per
+//                                           frontier edge, the edges split evenly over the grid
 //   kPullFrontier / kPullTopo ~ *_V_{Data,Topo}_Pull_* (BFS ..._V_Topo_Pull_..._Warp_...cu:57-79,
 //                                           CC_CUDA_V_Topo_Pull_..._Warp_...cu:59-78)
 //   kEdgeTopo  ~ *_E_Topo_Push_*            (BFS_CUDA_E_Topo_Push_..._Thread_...cu:57-72)
 //   kPushTopo  ~ *_V_Topo_Push_*            (BFS_CUDA_V_Topo_Push_..._Thread_...cu:56-79)
-// The B200 versions differ in mechanism, not in fixed point: frontier appends are
-// staged per block in shared memory and published with one global atomic per
-// round, duplicate pushes are filtered by a frontier bitmap (the reference uses
-// a `time[]` stamp array), adjacency is read with 128-bit loads, and vertices of
-// degree >= the heavy threshold are split into tiles shared by the whole grid.
+// The B200 versions differ in mechanism, not in fixed point:
+//  * frontier appends are staged per block in shared memory and published with
+//    one packed 64-bit atomic per flush, which also yields each entry's offset
+//    in the frontier's edge space (the reference appends with one atomicAdd per
+//    vertex, BFS_..._Warp_..._NonDup.cu:78);
+//  * duplicates are filtered by a frontier bitmap (the reference uses a time[]
+//    stamp array, :77);
+//  * each thread issues the dist[] loads of several neighbours before any of
+//    their atomicMin operations, so that several misses are in flight per thread;
+//  * adjacency is read with 128-bit loads where aligned, and the frontier's
+//    heavy vertices are cut into tiles that any block may take.
 #pragma once
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
 #include <cub/block/block_scan.cuh>
 #include "common.cuh"
 
@@ -25,101 +34,230 @@ namespace i2 {
 
 namespace cg = cooperative_groups;
 
-// Per-block staging of pushes into the next frontier.
-struct Stage {
-  int q[kQueue];
-  int hq[kHQueue];
-  int n;
-  int hn;
-  int base;
-  int hbase;
-  unsigned long long edges;
+constexpr int kScanItems = kQueue / kBlock;                 // staged entries per thread in a flush
+constexpr int kEdgesPerThread = 4;                          // edge-balanced variant
+constexpr int kTileEdges = kBlock * kEdgesPerThread;        // edges per edge-balanced tile
+
+typedef cub::BlockScan<int, kBlock> BlockScanT;
+
+// Frontier statistics of one thread's pushes; kept in registers and reduced
+// once per block at the end of the launch.
+struct Acc {
   int maxdeg;
   int mindist;
   int visited;
+};
+
+__device__ __forceinline__ void acc_init(Acc& a) {
+  a.maxdeg = 0;
+  a.mindist = kInf;
+  a.visited = 0;
+}
+
+// Per-block staging of pushes into the next frontier.
+struct Stage {
+  int q[kQueue];    // vertices
+  int qd[kQueue];   // their degrees
+  int hq[kHQueue];  // heavy vertices
+  int ht[kHQueue];  // their tile counts
+  int n;
+  int hn;
+  unsigned long long base;
+  unsigned long long hbase;
   int chunk;
   int last;
+  int j0;
+  int m;
+  Acc red[kBlock / kWarp];
+  typename BlockScanT::TempStorage scan;
 };
 
 __device__ __forceinline__ void stage_init(Stage& s) {
   if (threadIdx.x == 0) {
     s.n = 0;
     s.hn = 0;
-    s.edges = 0;
-    s.maxdeg = 0;
-    s.mindist = kInf;
-    s.visited = 0;
     s.last = 0;
   }
 }
 
-// Append a vertex to the next frontier, bypassing the staging queue. Used only
-// when a round produces more pushes than the shared queue holds.
-__device__ __forceinline__ void direct_append(int* counter, int* list, int v) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  int base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
-  base = g.shfl(base, 0);
-  list[base + g.thread_rank()] = v;
+__device__ __forceinline__ int heavy_tiles(int deg) { return (deg + kHeavyTile - 1) / kHeavyTile; }
+
+// Block-wide reduction of the per-thread statistics into s.red[0] (thread 0).
+// S is any shared struct with `Acc red[kBlock / kWarp]` and `int last`.
+template <typename S>
+__device__ __forceinline__ void acc_reduce(Acc a, S& s) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a.maxdeg = max(a.maxdeg, __shfl_down_sync(0xffffffffu, a.maxdeg, o));
+    a.mindist = min(a.mindist, __shfl_down_sync(0xffffffffu, a.mindist, o));
+    a.visited += __shfl_down_sync(0xffffffffu, a.visited, o);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s.red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      s.red[0].maxdeg = max(s.red[0].maxdeg, s.red[w].maxdeg);
+      s.red[0].mindist = min(s.red[0].mindist, s.red[w].mindist);
+      s.red[0].visited += s.red[w].visited;
+    }
+  }
 }
 
-// Record vertex v in the next frontier. The bitmap bit has already been
-// claimed by the caller, and the frontier minimum has already been updated.
-__device__ __forceinline__ void stage_vertex(const Ctx& c, Stage& s, int nxt, int v) {
-  const int beg = c.g.nindex[v];
-  const int deg = c.g.nindex[v + 1] - beg;
-  atomicAdd(&s.edges, (unsigned long long)deg);
-  atomicMax(&s.maxdeg, deg);
-  if (deg >= c.heavy) {
-    const int p = atomicAdd(&s.hn, 1);
-    if (p < kHQueue) s.hq[p] = v;
-    else direct_append(&c.ctl->slot[nxt].hsize, c.hwl[nxt], v);
+// Append (v, deg) or (v, tiles) to a list without the staging queue: used only
+// when a round produces more pushes than the shared queue holds. The threads
+// that overflow together share one packed atomic.
+__device__ __forceinline__ void direct_append(unsigned long long* packed, int* list, unsigned* off, int v, int w) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  const int pre = cg::exclusive_scan(g, w);
+  const int tot = cg::reduce(g, w, cg::plus<int>());
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(packed, ((unsigned long long)g.size() << 32) | (unsigned)tot);
+  base = g.shfl(base, 0);
+  const int pos = (int)(base >> 32) + (int)g.thread_rank();
+  list[pos] = v;
+  off[pos] = (unsigned)(base & 0xffffffffu) + (unsigned)pre;
+}
+
+// Record vertex v (degree deg >= 1) in the next frontier. The bitmap bit is
+// already set, and the frontier minimum already updated, by the caller.
+__device__ __forceinline__ void stage_entry(const Ctx& c, Stage& s, Acc& a, int nxt, int v, int deg) {
+  a.maxdeg = max(a.maxdeg, deg);
+  int p = atomicAdd(&s.n, 1);
+  if (p < kQueue) {
+    s.q[p] = v;
+    s.qd[p] = deg;
   } else {
-    const int p = atomicAdd(&s.n, 1);
-    if (p < kQueue) s.q[p] = v;
-    else direct_append(&c.ctl->slot[nxt].size, c.wl[nxt], v);
+    direct_append(&c.ctl->slot[nxt].packed, c.wl[nxt], c.woff[nxt], v, deg);
+  }
+  if (deg >= c.heavy) {
+    const int t = heavy_tiles(deg);
+    p = atomicAdd(&s.hn, 1);
+    if (p < kHQueue) {
+      s.hq[p] = v;
+      s.ht[p] = t;
+    } else {
+      direct_append(&c.ctl->slot[nxt].hpacked, c.hwl[nxt], c.htoff[nxt], v, t);
+    }
   }
 }
 
 // Push after a successful atomicMin (old > val). The frontier minimum is
 // lowered on every improvement, including repeat improvements of a vertex that
 // is already in the next frontier, so it is a true lower bound of the values
-// the next iteration reads.
-__device__ __forceinline__ void push_vertex(const Ctx& c, Stage& s, int nxt, int v, int val, int old) {
-  if (old == kInf) atomicAdd(&s.visited, 1);
-  atomicMin(&s.mindist, val);
+// the next iteration reads. A plain read of the bitmap word skips the atomic
+// for vertices already pushed in this launch (bits of the next frontier are
+// only set during the launch, so a set bit that is read is never stale).
+// Vertices without edges leave the frontier at once.
+__device__ __forceinline__ void push_vertex(const Ctx& c, Stage& s, Acc& a, int nxt, int v, int val, int old) {
+  if (old == kInf) a.visited++;
+  a.mindist = min(a.mindist, val);
   const unsigned bit = 1u << (v & 31);
-  if (atomicOr(&c.bm[nxt][v >> 5], bit) & bit) return;
-  stage_vertex(c, s, nxt, v);
+  unsigned* w = &c.bm[nxt][v >> 5];
+  if (*(volatile unsigned*)w & bit) return;
+  if (atomicOr(w, bit) & bit) return;
+  const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
+  if (deg == 0) {
+    atomicAnd(w, ~bit);
+    return;
+  }
+  stage_entry(c, s, a, nxt, v, deg);
 }
 
-// Publish the staged pushes of this block (block-uniform call).
+// Exclusive scan of up to kHQueue ints in shared memory by warp 0.
+__device__ __forceinline__ int warp_scan_heavy(Stage& s, int hn) {
+  constexpr int kPer = kHQueue / kWarp;
+  const int lane = threadIdx.x & 31;
+  int loc[kPer];
+  int sum = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int j = lane * kPer + i;
+    loc[i] = sum;
+    sum += j < hn ? s.ht[j] : 0;
+  }
+  int incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int excl = incl - sum;
+  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int j = lane * kPer + i;
+    if (j < hn) s.ht[j] = excl + loc[i];
+  }
+  return tot;
+}
+
+// Publish the staged pushes of this block (block-uniform call): one packed
+// atomic reserves positions and edge offsets for all staged entries.
 __device__ __forceinline__ void stage_flush(const Ctx& c, Stage& s, int nxt) {
   __syncthreads();
   const int n = min(s.n, kQueue);
   const int hn = min(s.hn, kHQueue);
   __syncthreads();  // every thread has read the counters before anyone changes them
   if (n == 0 && hn == 0) return;
-  if (threadIdx.x == 0) {
-    if (n) s.base = atomicAdd(&c.ctl->slot[nxt].size, n);
-    if (hn) s.hbase = atomicAdd(&c.ctl->slot[nxt].hsize, hn);
+  const int t = threadIdx.x;
+  int d[kScanItems];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int j = t * kScanItems + i;
+    d[i] = j < n ? s.qd[j] : 0;
+  }
+  int tot = 0;
+  BlockScanT(s.scan).ExclusiveSum(d, d, tot);
+  if (hn && t < 32) {
+    const int htot = warp_scan_heavy(s, hn);
+    if (t == 0) s.hbase = atomicAdd(&c.ctl->slot[nxt].hpacked, ((unsigned long long)hn << 32) | (unsigned)htot);
+  }
+  if (t == 0) {
+    if (n) s.base = atomicAdd(&c.ctl->slot[nxt].packed, ((unsigned long long)n << 32) | (unsigned)tot);
     s.n = 0;
     s.hn = 0;
   }
   __syncthreads();
-  int* wl = c.wl[nxt];
-  for (int j = threadIdx.x; j < n; j += blockDim.x) wl[s.base + j] = s.q[j];
-  int* hwl = c.hwl[nxt];
-  for (int j = threadIdx.x; j < hn; j += blockDim.x) hwl[s.hbase + j] = s.hq[j];
+  if (n) {
+    const int b = (int)(s.base >> 32);
+    const unsigned eb = (unsigned)(s.base & 0xffffffffu);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const int j = t * kScanItems + i;
+      if (j < n) {
+        c.wl[nxt][b + j] = s.q[j];
+        c.woff[nxt][b + j] = eb + (unsigned)d[i];
+      }
+    }
+  }
+  if (hn) {
+    const int b = (int)(s.hbase >> 32);
+    const unsigned tb = (unsigned)(s.hbase & 0xffffffffu);
+    for (int j = t; j < hn; j += blockDim.x) {
+      c.hwl[nxt][b + j] = s.hq[j];
+      c.htoff[nxt][b + j] = tb + (unsigned)s.ht[j];
+    }
+  }
   __syncthreads();
 }
 
-template <int ALG>
-__device__ __forceinline__ void relax_edge(const Ctx& c, Stage& s, int nxt, int du, int v, int w) {
-  const int cand = Op<ALG>::cand(du, w);
-  if (cand < c.dist[v]) {
-    const int old = atomicMin(&c.dist[v], cand);
-    if (cand < old) push_vertex(c, s, nxt, v, cand, old);
+// Relax up to R candidate edges of this thread. All dist[] loads are issued
+// before any atomicMin. A value read before another thread lowered it is only
+// larger, which can cost an unneeded atomic but never skips an improvement.
+template <int ALG, int R>
+__device__ __forceinline__ void relax_batch(const Ctx& c, Stage& s, Acc& a, int nxt, const int* du, const int* nv,
+                                            const int* wv, const bool* ok) {
+  int cand[R], cur[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    cand[r] = ok[r] ? Op<ALG>::cand(du[r], wv[r]) : kInf;
+    cur[r] = ok[r] ? c.dist[nv[r]] : kInf;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (cand[r] < cur[r]) {
+      const int old = atomicMin(&c.dist[nv[r]], cand[r]);
+      if (cand[r] < old) push_vertex(c, s, a, nxt, nv[r], cand[r], old);
+    }
   }
 }
 
@@ -128,99 +266,157 @@ __device__ __forceinline__ void relax_edge(const Ctx& c, Stage& s, int nxt, int 
 // (and eweight) are read with one 128-bit load; a unit that would reach past
 // the end of the arrays is read element by element.
 template <int ALG>
-__device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, int nxt, int du, int lo, int hi,
-                                            int lane, int gsize) {
+__device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int nxt, int du, int lo, int hi, int lane,
+                                            int gsize) {
   const int* __restrict__ nl = c.g.nlist;
   const int* __restrict__ ew = c.g.eweight;
+  const int dus[4] = {du, du, du, du};
   if (c.g.vec_ok && hi - lo >= 8) {
     const int q0 = lo >> 2;
     const int q1 = (hi + 3) >> 2;
     for (int q = q0 + lane; q < q1; q += gsize) {
       const int k0 = q << 2;
       int nv[4], wv[4] = {0, 0, 0, 0};
+      bool ok[4];
       if (k0 + 3 < c.g.edges) {
-        const int4 a = __ldg(reinterpret_cast<const int4*>(nl + k0));
-        nv[0] = a.x; nv[1] = a.y; nv[2] = a.z; nv[3] = a.w;
+        const int4 x = __ldg(reinterpret_cast<const int4*>(nl + k0));
+        nv[0] = x.x; nv[1] = x.y; nv[2] = x.z; nv[3] = x.w;
         if (Op<ALG>::kWeighted) {
-          const int4 b = __ldg(reinterpret_cast<const int4*>(ew + k0));
-          wv[0] = b.x; wv[1] = b.y; wv[2] = b.z; wv[3] = b.w;
+          const int4 y = __ldg(reinterpret_cast<const int4*>(ew + k0));
+          wv[0] = y.x; wv[1] = y.y; wv[2] = y.z; wv[3] = y.w;
         }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ok[r] = k0 + r >= lo && k0 + r < hi;
       } else {
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int k = k0 + t;
-          nv[t] = (k >= lo && k < hi) ? nl[k] : 0;
-          if (Op<ALG>::kWeighted) wv[t] = (k >= lo && k < hi) ? ew[k] : 0;
+        for (int r = 0; r < 4; ++r) {
+          const int k = k0 + r;
+          ok[r] = k >= lo && k < hi;
+          nv[r] = ok[r] ? nl[k] : 0;
+          if (Op<ALG>::kWeighted) wv[r] = ok[r] ? ew[k] : 0;
         }
       }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int k = k0 + t;
-        if (k >= lo && k < hi) relax_edge<ALG>(c, s, nxt, du, nv[t], wv[t]);
-      }
+      relax_batch<ALG, 4>(c, s, a, nxt, dus, nv, wv, ok);
     }
   } else {
-    for (int k = lo + lane; k < hi; k += gsize) {
-      const int w = Op<ALG>::kWeighted ? __ldg(ew + k) : 0;
-      relax_edge<ALG>(c, s, nxt, du, __ldg(nl + k), w);
+    for (int k0 = lo + lane * 4; k0 < hi; k0 += gsize * 4) {
+      int nv[4], wv[4] = {0, 0, 0, 0};
+      bool ok[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = k0 + r;
+        ok[r] = k < hi;
+        nv[r] = ok[r] ? __ldg(nl + k) : 0;
+        if (Op<ALG>::kWeighted) wv[r] = ok[r] ? __ldg(ew + k) : 0;
+      }
+      relax_batch<ALG, 4>(c, s, a, nxt, dus, nv, wv, ok);
     }
   }
 }
 
+// Last j in [0, n) with off[j] <= x (off[0] == 0 <= x).
+__device__ __forceinline__ int owner_search(const unsigned* __restrict__ off, int n, unsigned x) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Warp-cooperative version for global arrays (warp 0 calls it; every lane gets
+// the result): each round probes 32 evenly spaced positions, so the range
+// shrinks 32-fold per round of parallel loads instead of 2-fold per dependent load.
+__device__ __forceinline__ int owner_search_warp(const unsigned* __restrict__ off, int n, unsigned x) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = n;  // off[lo] <= x, answer in [lo, hi)
+  while (hi - lo > 32) {
+    const long long span = hi - lo;
+    const int p = lo + (int)((span * lane) / 32);
+    const unsigned ballot = __ballot_sync(0xffffffffu, off[p] <= x);
+    const int last = 31 - __clz(ballot);  // lane 0 always qualifies (p == lo)
+    const int nlo = lo + (int)((span * last) / 32);
+    const int nhi = last == 31 ? hi : lo + (int)((span * (last + 1)) / 32);
+    lo = nlo;
+    hi = nhi;
+  }
+  const int p = lo + lane;
+  const unsigned ballot = __ballot_sync(0xffffffffu, p < hi && off[p] <= x);
+  return lo + 31 - __clz(ballot);
+}
+
+// Flush only when the staging queue is at least half full (block-uniform).
+__device__ __forceinline__ void stage_flush_if_half(const Ctx& c, Stage& s, int nxt) {
+  __syncthreads();
+  const bool full = s.n >= kQueue / 2 || s.hn >= kHQueue / 2;
+  __syncthreads();
+  if (full) stage_flush(c, s, nxt);
+}
+
+// Contiguous share [lo, hi) of [0, total) for this block.
+__device__ __forceinline__ void block_share(unsigned total, unsigned* lo, unsigned* hi) {
+  *lo = (unsigned)(((unsigned long long)total * blockIdx.x) / gridDim.x);
+  *hi = (unsigned)(((unsigned long long)total * (blockIdx.x + 1)) / gridDim.x);
+}
+
 // Heavy frontier vertices: their adjacency is cut into tiles of kHeavyTile
-// entries, and tile t of the concatenated tile sequence goes to block t % grid.
+// entries. Each block takes a contiguous share of the tile sequence, finds the
+// vertex of its first tile once, and walks forward.
 template <int ALG>
-__device__ void heavy_path(const Ctx& c, Stage& s, int cur, int nxt) {
-  const int nh = c.ctl->slot[cur].hsize;
-  const int G = gridDim.x;
-  long long tbase = 0;
-  for (int j = 0; j < nh; ++j) {
+__device__ void heavy_path(const Ctx& c, Stage& s, Acc& a, int cur, int nxt) {
+  const unsigned long long hp = c.ctl->slot[cur].hpacked;
+  const int nh = slot_size(hp);
+  const unsigned ntiles = slot_edges(hp);
+  if (ntiles == 0) return;
+  unsigned t0, t1;
+  block_share(ntiles, &t0, &t1);
+  if (t0 >= t1) return;  // uniform
+  const unsigned* __restrict__ toff = c.htoff[cur];
+  if (threadIdx.x < 32) {
+    const int j = owner_search_warp(toff, nh, t0);
+    if (threadIdx.x == 0) s.j0 = j;
+  }
+  __syncthreads();
+  int j = s.j0;
+  for (unsigned t = t0; t < t1; ++t) {
+    while (j + 1 < nh && toff[j + 1] <= t) ++j;
     const int u = c.hwl[cur][j];
     const int du = c.dist[u];
     const int beg = c.g.nindex[u];
     const int end = c.g.nindex[u + 1];
-    const int ntiles = (end - beg + kHeavyTile - 1) / kHeavyTile;
-    if (Op<ALG>::valid(du)) {
-      int t = (int)(((long long)blockIdx.x - (tbase % G) + G) % G);
-      for (; t < ntiles; t += G) {
-        const int lo = beg + t * kHeavyTile;
-        const int hi = min(end, lo + kHeavyTile);
-        relax_range<ALG>(c, s, nxt, du, lo, hi, threadIdx.x, blockDim.x);
-        stage_flush(c, s, nxt);
-      }
-    }
-    tbase += ntiles;
+    const int lo = beg + (int)(t - toff[j]) * kHeavyTile;
+    const int hi = min(end, lo + kHeavyTile);
+    if (Op<ALG>::valid(du)) relax_range<ALG>(c, s, a, nxt, du, lo, hi, threadIdx.x, blockDim.x);
+    stage_flush_if_half(c, s, nxt);
   }
 }
 
 // Clear the bitmap of F_{i-1} (slot old): by entries when it is small, by words otherwise.
 __device__ __forceinline__ void clear_old(const Ctx& c, int old) {
-  const int n = c.ctl->slot[old].size;
-  const int hn = c.ctl->slot[old].hsize;
+  const int n = slot_size(c.ctl->slot[old].packed);
   unsigned* bm = c.bm[old];
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if ((long long)(n + hn) * 4 > c.bm_words) {
+  if ((long long)n * 4 > c.bm_words) {
     for (long long w = tid; w < c.bm_words; w += stride) bm[w] = 0u;
   } else {
     const int* wl = c.wl[old];
     for (long long j = tid; j < n; j += stride) bm[wl[j] >> 5] = 0u;
-    const int* hwl = c.hwl[old];
-    for (long long j = tid; j < hn; j += stride) bm[hwl[j] >> 5] = 0u;
   }
 }
 
 __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old);
 
 // Common epilogue: publish block statistics and let the last block finish the iteration.
-__device__ __forceinline__ void block_epilogue(const Ctx& c, Stage& s, int i, int cur, int nxt, int old) {
-  __syncthreads();
+template <typename S>
+__device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a, int i, int cur, int nxt, int old) {
+  acc_reduce(a, s);
   if (threadIdx.x == 0) {
+    const Acc& r = s.red[0];
     Slot& sl = c.ctl->slot[nxt];
-    if (s.edges) atomicAdd(&sl.edges, s.edges);
-    if (s.maxdeg) atomicMax(&sl.maxdeg, s.maxdeg);
-    if (s.mindist != kInf) atomicMin(&sl.mindist, s.mindist);
-    if (s.visited) atomicAdd((unsigned long long*)&c.ctl->visited, (unsigned long long)s.visited);
+    if (r.maxdeg) atomicMax(&sl.maxdeg, r.maxdeg);
+    if (r.mindist != kInf) atomicMin(&sl.mindist, r.mindist);
+    if (r.visited) atomicAdd((unsigned long long*)&c.ctl->visited, (unsigned long long)r.visited);
     __threadfence();
     const unsigned t = atomicAdd(&c.ctl->done, 1u);
     s.last = (t == gridDim.x - 1);
@@ -237,29 +433,26 @@ __device__ __forceinline__ void block_prologue(const Ctx& c) {
 }
 
 // ---------------------------------------------------------------------------
-// Data-driven push variants.
+// Data-driven push, vertex granularity: thread, warp or block per frontier
+// vertex. Heavy vertices are skipped here and taken by the heavy path.
 
 template <int ALG, int VAR>
 __global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
   __shared__ Stage s;
-  typedef cub::BlockScan<int, kBlock> Scan;
-  __shared__ typename Scan::TempStorage scan_tmp;
-  __shared__ int s_beg[kBlock];
-  __shared__ int s_off[kBlock + 1];
-  __shared__ int s_du[kBlock];
-
   block_prologue(c);
   stage_init(s);
+  Acc a;
+  acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
   clear_old(c, old);
   __syncthreads();
 
-  const int n = c.ctl->slot[cur].size;
+  const int n = slot_size(c.ctl->slot[cur].packed);
   const int* __restrict__ wl = c.wl[cur];
-  const int per = (VAR == kVPThread || VAR == kVPCta) ? kBlock : (VAR == kVPWarp ? kBlock / kWarp : 1);
+  const int per = VAR == kVPThread ? kBlock : (VAR == kVPWarp ? kBlock / kWarp : 1);
 
-  while (true) {
+  for (;;) {
     if (threadIdx.x == 0) s.chunk = atomicAdd(&c.ctl->chunk, per);
     __syncthreads();
     const int base = s.chunk;
@@ -268,56 +461,233 @@ __global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
       const int idx = base + threadIdx.x;
       if (idx < n) {
         const int u = wl[idx];
+        const int beg = c.g.nindex[u], end = c.g.nindex[u + 1];
         const int du = c.dist[u];
-        if (Op<ALG>::valid(du)) relax_range<ALG>(c, s, nxt, du, c.g.nindex[u], c.g.nindex[u + 1], 0, 1);
+        if (end - beg < c.heavy && Op<ALG>::valid(du)) relax_range<ALG>(c, s, a, nxt, du, beg, end, 0, 1);
       }
     } else if (VAR == kVPWarp) {
       const int idx = base + threadIdx.x / kWarp;
       if (idx < n) {
         const int u = wl[idx];
+        const int beg = c.g.nindex[u], end = c.g.nindex[u + 1];
         const int du = c.dist[u];
-        if (Op<ALG>::valid(du))
-          relax_range<ALG>(c, s, nxt, du, c.g.nindex[u], c.g.nindex[u + 1], threadIdx.x % kWarp, kWarp);
+        if (end - beg < c.heavy && Op<ALG>::valid(du))
+          relax_range<ALG>(c, s, a, nxt, du, beg, end, threadIdx.x % kWarp, kWarp);
       }
-    } else if (VAR == kVPBlock) {
+    } else {
       const int u = wl[base];
+      const int beg = c.g.nindex[u], end = c.g.nindex[u + 1];
       const int du = c.dist[u];
-      if (Op<ALG>::valid(du))
-        relax_range<ALG>(c, s, nxt, du, c.g.nindex[u], c.g.nindex[u + 1], threadIdx.x, blockDim.x);
-    } else {  // kVPCta: scan the degrees of a chunk, then one thread per edge
-      const int idx = base + threadIdx.x;
-      int deg = 0, beg = 0, du = kInf;
-      if (idx < n) {
-        const int u = wl[idx];
-        du = c.dist[u];
-        beg = c.g.nindex[u];
-        deg = Op<ALG>::valid(du) ? c.g.nindex[u + 1] - beg : 0;
-      }
-      int off, total;
-      Scan(scan_tmp).ExclusiveSum(deg, off, total);
-      s_beg[threadIdx.x] = beg;
-      s_off[threadIdx.x] = off;
-      s_du[threadIdx.x] = du;
-      if (threadIdx.x == 0) s_off[kBlock] = total;
-      __syncthreads();
-      const int* __restrict__ nl = c.g.nlist;
-      const int* __restrict__ ew = c.g.eweight;
-      for (int k = threadIdx.x; k < total; k += kBlock) {
-        int lo = 0, hi = kBlock;  // find j with s_off[j] <= k < s_off[j+1]
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (s_off[mid] <= k) lo = mid; else hi = mid;
-        }
-        const int e = s_beg[lo] + (k - s_off[lo]);
-        const int w = Op<ALG>::kWeighted ? __ldg(ew + e) : 0;
-        relax_edge<ALG>(c, s, nxt, s_du[lo], __ldg(nl + e), w);
-      }
+      if (end - beg < c.heavy && Op<ALG>::valid(du))
+        relax_range<ALG>(c, s, a, nxt, du, beg, end, threadIdx.x, blockDim.x);
     }
-    stage_flush(c, s, nxt);
+    stage_flush_if_half(c, s, nxt);
   }
-  heavy_path<ALG>(c, s, cur, nxt);
+  heavy_path<ALG>(c, s, a, cur, nxt);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old);
+}
+
+// ---------------------------------------------------------------------------
+// Edge-balanced push: the frontier's edges [0, edges) are split into one
+// contiguous share per warp of the grid (equal edges, hence equal work). A warp
+// finds the frontier entry holding its first edge once (warp-cooperative
+// search) and walks its share in warp tiles of kWarpTile edges: it loads the
+// entries overlapping the tile into its own slice of shared memory, and each
+// lane relaxes kEdgesPerThread consecutive edges. Warps never wait for each
+// other: each stages its pushes in its own queue and publishes them with a
+// warp scan and one packed atomic. No vertex is too big or too small: work is
+// split by edges, as in the reference's edge-centric codes.
+constexpr int kWarpTile = kWarp * kEdgesPerThread;  // edges per warp tile
+constexpr int kWarpQueue = 2 * kWarpTile;           // warp staging capacity
+constexpr int kWarpsPerBlock = kBlock / kWarp;
+
+struct WarpStage {
+  unsigned off[kWarpTile + kWarp];
+  int beg[kWarpTile];
+  int du[kWarpTile];
+  int q[kWarpQueue];
+  int qd[kWarpQueue];
+  int n;
+};
+
+// Stage a push into the warp's queue (heavy entries go straight to their list).
+__device__ __forceinline__ void warp_stage_entry(const Ctx& c, WarpStage& ws, Acc& a, int nxt, int v, int deg) {
+  a.maxdeg = max(a.maxdeg, deg);
+  const int p = atomicAdd(&ws.n, 1);
+  if (p < kWarpQueue) {
+    ws.q[p] = v;
+    ws.qd[p] = deg;
+  } else {
+    direct_append(&c.ctl->slot[nxt].packed, c.wl[nxt], c.woff[nxt], v, deg);
+  }
+  if (deg >= c.heavy) direct_append(&c.ctl->slot[nxt].hpacked, c.hwl[nxt], c.htoff[nxt], v, heavy_tiles(deg));
+}
+
+__device__ __forceinline__ void warp_push_vertex(const Ctx& c, WarpStage& ws, Acc& a, int nxt, int v, int val,
+                                                 int old) {
+  if (old == kInf) a.visited++;
+  a.mindist = min(a.mindist, val);
+  const unsigned bit = 1u << (v & 31);
+  unsigned* w = &c.bm[nxt][v >> 5];
+  if (*(volatile unsigned*)w & bit) return;
+  if (atomicOr(w, bit) & bit) return;
+  const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
+  if (deg == 0) {
+    atomicAnd(w, ~bit);
+    return;
+  }
+  warp_stage_entry(c, ws, a, nxt, v, deg);
+}
+
+// Publish the warp's staged entries (warp-uniform call).
+__device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt) {
+  constexpr int kPer = kWarpQueue / kWarp;
+  __syncwarp();
+  const int n = min(ws.n, kWarpQueue);
+  __syncwarp();
+  if (n == 0) return;
+  const int lane = threadIdx.x & 31;
+  int d[kPer];
+  int sum = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int j = lane * kPer + i;
+    d[i] = sum;
+    sum += j < n ? ws.qd[j] : 0;
+  }
+  int incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int excl = incl - sum;
+  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(&c.ctl->slot[nxt].packed, ((unsigned long long)n << 32) | (unsigned)tot);
+    ws.n = 0;
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const int b = (int)(base >> 32);
+  const unsigned eb = (unsigned)(base & 0xffffffffu);
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int j = lane * kPer + i;
+    if (j < n) {
+      c.wl[nxt][b + j] = ws.q[j];
+      c.woff[nxt][b + j] = eb + (unsigned)(excl + d[i]);
+    }
+  }
+  __syncwarp();
+}
+
+template <int ALG>
+__device__ __forceinline__ void warp_relax_batch(const Ctx& c, WarpStage& ws, Acc& a, int nxt, const int* du,
+                                                 const int* nv, const int* wv, const bool* ok) {
+  int cand[kEdgesPerThread], cur[kEdgesPerThread];
+#pragma unroll
+  for (int r = 0; r < kEdgesPerThread; ++r) {
+    cand[r] = ok[r] ? Op<ALG>::cand(du[r], wv[r]) : kInf;
+    cur[r] = ok[r] ? c.dist[nv[r]] : kInf;
+  }
+#pragma unroll
+  for (int r = 0; r < kEdgesPerThread; ++r) {
+    if (cand[r] < cur[r]) {
+      const int old = atomicMin(&c.dist[nv[r]], cand[r]);
+      if (cand[r] < old) warp_push_vertex(c, ws, a, nxt, nv[r], cand[r], old);
+    }
+  }
+}
+
+struct EpiStage {
+  Acc red[kBlock / kWarp];
+  int last;
+};
+
+// Minimum resident blocks per SM the edge-balanced kernel is compiled for
+// (bounds its registers: 6 -> 40 per thread).
+#ifndef I2_EB_MIN_BLOCKS
+#define I2_EB_MIN_BLOCKS 6
+#endif
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(Ctx c) {
+  __shared__ EpiStage s;
+  __shared__ WarpStage wss[kWarpsPerBlock];
+  block_prologue(c);
+  if (threadIdx.x == 0) s.last = 0;
+  Acc a;
+  acc_init(a);
+  const int i = c.ctl->iter;
+  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
+  clear_old(c, old);
+  const int lane = threadIdx.x & 31;
+  WarpStage& ws = wss[threadIdx.x >> 5];
+  if (lane == 0) ws.n = 0;
+  __syncwarp();
+
+  const unsigned long long P = c.ctl->slot[cur].packed;
+  const int n = slot_size(P);
+  const unsigned total = slot_edges(P);
+  const int* __restrict__ wl = c.wl[cur];
+  const unsigned* __restrict__ woff = c.woff[cur];
+  const int* __restrict__ nl = c.g.nlist;
+  const int* __restrict__ ew = c.g.eweight;
+  const unsigned long long gw = (unsigned long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const unsigned long long nw = (unsigned long long)gridDim.x * kWarpsPerBlock;
+  const unsigned W0 = (unsigned)((total * gw) / nw);
+  const unsigned W1 = (unsigned)((total * (gw + 1)) / nw);
+  if (W0 < W1) {
+    int j = owner_search_warp(woff, n, W0);  // entry holding edge W0
+    for (unsigned e0 = W0; e0 < W1; e0 += kWarpTile) {
+      const unsigned e1 = min(W1, e0 + kWarpTile);
+      // offsets of the entries from j on, 32 at a time, until one reaches e1
+      int m = 0;
+      for (;;) {
+        const int jj = j + m + lane;
+        const unsigned w = jj < n ? woff[jj] : total;
+        ws.off[m + lane] = w;
+        const int below = __popc(__ballot_sync(0xffffffffu, w < e1));
+        m += below;
+        if (below < kWarp) break;
+      }
+      for (int k = lane; k < m; k += kWarp) {
+        const int v = wl[j + k];
+        ws.beg[k] = c.g.nindex[v];
+        ws.du[k] = c.dist[v];
+      }
+      __syncwarp();
+      const unsigned x0 = e0 + (unsigned)lane * kEdgesPerThread;
+      int du[kEdgesPerThread], nv[kEdgesPerThread], wv[kEdgesPerThread];
+      bool ok[kEdgesPerThread];
+      int o = x0 < e1 ? owner_search(ws.off, m, x0) : 0;
+#pragma unroll
+      for (int r = 0; r < kEdgesPerThread; ++r) {
+        const unsigned x = x0 + r;
+        ok[r] = x < e1;
+        nv[r] = 0;
+        wv[r] = 0;
+        du[r] = kInf;
+        if (ok[r]) {
+          while (x >= ws.off[o + 1]) ++o;
+          const int e = ws.beg[o] + (int)(x - ws.off[o]);
+          nv[r] = __ldg(nl + e);
+          if (Op<ALG>::kWeighted) wv[r] = __ldg(ew + e);
+          du[r] = ws.du[o];
+          ok[r] = Op<ALG>::valid(du[r]);
+        }
+      }
+      warp_relax_batch<ALG>(c, ws, a, nxt, du, nv, wv, ok);
+      // the next tile starts at e1: its first entry is the last one with offset <= e1
+      j += (ws.off[m] == e1) ? m : m - 1;
+      __syncwarp();
+      if (ws.n >= kWarpQueue - kWarpTile) warp_flush(c, ws, nxt);
+    }
+  }
+  warp_flush(c, ws, nxt);
+  __syncthreads();
+  block_epilogue(c, s, a, i, cur, nxt, old);
 }
 
 // ---------------------------------------------------------------------------
@@ -328,6 +698,8 @@ __global__ void __launch_bounds__(kBlock) relax_push_topo(Ctx c) {
   __shared__ Stage s;
   block_prologue(c);
   stage_init(s);
+  Acc a;
+  acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
   clear_old(c, old);
@@ -340,13 +712,13 @@ __global__ void __launch_bounds__(kBlock) relax_push_topo(Ctx c) {
       const int beg = c.g.nindex[v];
       const int end = c.g.nindex[v + 1];
       const int du = c.dist[v];
-      if (end - beg < c.heavy && Op<ALG>::valid(du)) relax_range<ALG>(c, s, nxt, du, beg, end, 0, 1);
+      if (end - beg < c.heavy && Op<ALG>::valid(du)) relax_range<ALG>(c, s, a, nxt, du, beg, end, 0, 1);
     }
-    stage_flush(c, s, nxt);
+    stage_flush_if_half(c, s, nxt);
   }
-  heavy_path<ALG>(c, s, cur, nxt);
+  heavy_path<ALG>(c, s, a, cur, nxt);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old);
 }
 
 // ---------------------------------------------------------------------------
@@ -356,6 +728,8 @@ __global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
   __shared__ Stage s;
   block_prologue(c);
   stage_init(s);
+  Acc a;
+  acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
   clear_old(c, old);
@@ -370,38 +744,40 @@ __global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
     const long long q = base + threadIdx.x;
     if (q < units) {
       const long long k0 = q << 2;
-      int su[4], nv[4], wv[4] = {0, 0, 0, 0};
+      int su[4], nv[4], wv[4] = {0, 0, 0, 0}, du[4];
+      bool ok[4];
       if (c.g.vec_ok && k0 + 3 < E) {
-        const int4 a = __ldg(reinterpret_cast<const int4*>(sp + k0));
-        su[0] = a.x; su[1] = a.y; su[2] = a.z; su[3] = a.w;
-        const int4 b = __ldg(reinterpret_cast<const int4*>(nl + k0));
-        nv[0] = b.x; nv[1] = b.y; nv[2] = b.z; nv[3] = b.w;
+        const int4 x = __ldg(reinterpret_cast<const int4*>(sp + k0));
+        su[0] = x.x; su[1] = x.y; su[2] = x.z; su[3] = x.w;
+        const int4 y = __ldg(reinterpret_cast<const int4*>(nl + k0));
+        nv[0] = y.x; nv[1] = y.y; nv[2] = y.z; nv[3] = y.w;
         if (Op<ALG>::kWeighted) {
-          const int4 d = __ldg(reinterpret_cast<const int4*>(ew + k0));
-          wv[0] = d.x; wv[1] = d.y; wv[2] = d.z; wv[3] = d.w;
+          const int4 z = __ldg(reinterpret_cast<const int4*>(ew + k0));
+          wv[0] = z.x; wv[1] = z.y; wv[2] = z.z; wv[3] = z.w;
         }
       } else {
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const long long k = k0 + t;
-          su[t] = (k < E) ? sp[k] : -1;
-          nv[t] = (k < E) ? nl[k] : 0;
-          if (Op<ALG>::kWeighted) wv[t] = (k < E) ? ew[k] : 0;
+        for (int r = 0; r < 4; ++r) {
+          const long long k = k0 + r;
+          su[r] = (k < E) ? sp[k] : -1;
+          nv[r] = (k < E) ? nl[k] : 0;
+          if (Op<ALG>::kWeighted) wv[r] = (k < E) ? ew[k] : 0;
         }
       }
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int u = su[t];
-        if (u >= 0 && ((bmc[u >> 5] >> (u & 31)) & 1u)) {
-          const int du = c.dist[u];
-          if (Op<ALG>::valid(du)) relax_edge<ALG>(c, s, nxt, du, nv[t], wv[t]);
-        }
+      for (int r = 0; r < 4; ++r) {
+        const int u = su[r];
+        ok[r] = u >= 0 && ((bmc[u >> 5] >> (u & 31)) & 1u);
+        du[r] = ok[r] ? c.dist[u] : kInf;
       }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) ok[r] = ok[r] && Op<ALG>::valid(du[r]);
+      relax_batch<ALG, 4>(c, s, a, nxt, du, nv, wv, ok);
     }
-    stage_flush(c, s, nxt);
+    stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old);
 }
 
 // ---------------------------------------------------------------------------
@@ -414,6 +790,8 @@ __global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
   __shared__ Stage s;
   block_prologue(c);
   stage_init(s);
+  Acc a;
+  acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
   clear_old(c, old);
@@ -428,13 +806,14 @@ __global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
   for (long long base = (long long)blockIdx.x * kBlock; base < V; base += (long long)gridDim.x * kBlock) {
     const int v = (int)base + threadIdx.x;
     bool improved = false;
-    int best = kInf, dv = kInf;
+    int best = kInf, dv = kInf, deg = 0;
     if (v < V) {
       dv = c.dist[v];
       best = dv;
       if (!FRONTIER || dv > bound) {
         const int beg = c.g.nindex[v];
         const int end = c.g.nindex[v + 1];
+        deg = end - beg;
         for (int k = beg; k < end; ++k) {
           const int u = __ldg(nl + k);
           if (FRONTIER && !((bmc[u >> 5] >> (u & 31)) & 1u)) continue;
@@ -456,14 +835,14 @@ __global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
     const unsigned word = __ballot_sync(0xffffffffu, improved);
     if ((threadIdx.x & 31) == 0 && word) c.bm[nxt][v >> 5] = word;
     if (improved) {
-      if (dv == kInf) atomicAdd(&s.visited, 1);
-      atomicMin(&s.mindist, best);
-      stage_vertex(c, s, nxt, v);
+      if (dv == kInf) a.visited++;
+      a.mindist = min(a.mindist, best);
+      stage_entry(c, s, a, nxt, v, deg);
     }
-    stage_flush(c, s, nxt);
+    stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old);
 }
 
 }  // namespace i2
