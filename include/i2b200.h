@@ -36,7 +36,8 @@ typedef enum {
   I2_ERR_NO_DEVICE = 6,   /* no CUDA device */
   I2_ERR_UNSUPPORTED = 7, /* variant not applicable to this graph (pull on a directed graph) */
   I2_ERR_ITER_CAP = 8,    /* iteration cap reached before the fixed point */
-  I2_ERR_OVERFLOW = 9     /* int32 limit or capacity exceeded */
+  I2_ERR_OVERFLOW = 9,    /* int32 limit or capacity exceeded */
+  I2_ERR_CAPACITY = 10    /* graph larger than i2_run_noalloc's fixed scratch */
 } i2_status;
 
 /* Host CSR graph. Layout-identical to struct ECLgraph (include/ECLgraph.h:44-50). */
@@ -203,6 +204,22 @@ int i2_mlp_train(float* params, const float* X, const float* T, const float* M, 
                  int batch, float lr, uint64_t seed, float* final_loss);
 /* Device inference on n feature rows; writes the chosen variant per row (mask of allowed variants). */
 int i2_mlp_predict(const float* params, const float* X, int n, int allowed_mask, int* choice);
+
+/* ---- traversal that allocates nothing ----
+   No counterpart in the reference. For callers that cannot allocate device
+   memory when they query (device memory held by another allocator, query loops
+   that cannot afford cudaMalloc's device synchronisation, or no tolerance for
+   out-of-memory at query time). The caller passes the CSR and the output
+   `dist_dev` (nodes ints), all in device memory; the scratch is a fixed device
+   array inside the library (about 3 MB, held on every GPU that loads the
+   library until exit), so graphs above 131072 vertices return I2_ERR_CAPACITY.
+   Style: edge-balanced push, host-driven loop on `stream` (NULL: legacy
+   stream). The first call on each device looks up the scratch's device
+   address; make that first call before any stream capture. All calls share the
+   one scratch: calls that overlap on the GPU (other streams, other host
+   threads) race and must be serialised by the caller. src is ignored for
+   I2_CC. `iterations` may be NULL. */
+int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* dist_dev, void* stream, int* iterations);
 
 /* ---- batches of graphs traversed together ---- */
 typedef struct i2_batch i2_batch;

@@ -21,6 +21,7 @@ I2_ERR_NO_DEVICE = 6
 I2_ERR_UNSUPPORTED = 7
 I2_ERR_ITER_CAP = 8
 I2_ERR_OVERFLOW = 9
+I2_ERR_CAPACITY = 10
 
 I2_BFS, I2_SSSP, I2_CC = 0, 1, 2
 
@@ -104,6 +105,7 @@ SIGNATURES = {
     "i2_mlp_loss_grad": (_I, [_PF, _PF, _PF, _PF, _I, _PF, _PF]),
     "i2_mlp_train": (_I, [_PF, _PF, _PF, _PF, _I, _I, _I, C.c_float, C.c_uint64, _PF]),
     "i2_mlp_predict": (_I, [_PF, _PF, _I, _I, _PI]),
+    "i2_run_noalloc": (_I, [_I, _PG, _I, C.c_void_p, C.c_void_p, _PI]),
     "i2_batch_upload": (_I, [_PG, _I, C.POINTER(_P)]),
     "i2_batch_run": (_I, [_P, _I, _PI, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_batch_offsets": (_I, [_P, C.POINTER(C.c_longlong)]),

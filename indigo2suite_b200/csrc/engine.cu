@@ -1061,6 +1061,7 @@ const char* i2_status_string(int status) {
     case I2_ERR_UNSUPPORTED: return "variant not supported on this graph";
     case I2_ERR_ITER_CAP: return "iteration cap reached";
     case I2_ERR_OVERFLOW: return "int32 limit exceeded";
+    case I2_ERR_CAPACITY: return "graph exceeds the fixed scratch of i2_run_noalloc";
   }
   return "unknown status";
 }
@@ -1358,3 +1359,156 @@ int i2_mlp_param_count(void) { return kParams; }
 int i2_mlp_set_params(const float* params, int count) { return mlp_install(params, count); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Traversal that allocates nothing.
+//
+// Some callers cannot allocate device memory at the moment they run a query:
+// their process's device memory is already held by another allocator (for
+// example a framework's caching allocator that reserved the GPU), their query
+// loop cannot afford cudaMalloc/cudaFree, which synchronise the device, or
+// their query must not be able to fail with out-of-memory. i2_run_noalloc
+// serves them: the caller passes the CSR arrays and the output array (all in
+// device memory), and every piece of scratch the traversal needs (frontier
+// lists, their edge offsets, the frontier bitmaps and the control block) lives
+// in one fixed-size device array defined in this file. That array is part of
+// the library image: every GPU that loads the library holds it (about 3 MB)
+// until the process exits. Graphs above kNoAllocMaxNodes vertices are refused.
+
+namespace i2 {
+
+constexpr int kNoAllocMaxNodes = 1 << 17;  // 131072 vertices
+constexpr int kNoAllocWords = kNoAllocMaxNodes / 32;
+
+// Layout of the scratch array (offsets in bytes, each 256-byte aligned).
+constexpr size_t kNoAllocAlign(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaWl = 0;
+constexpr size_t kNaWoff = kNaWl + kNoAllocAlign(3ull * kNoAllocMaxNodes * sizeof(int));
+constexpr size_t kNaBm = kNaWoff + kNoAllocAlign(3ull * kNoAllocMaxNodes * sizeof(unsigned));
+constexpr size_t kNaHeavy = kNaBm + kNoAllocAlign(3ull * kNoAllocWords * sizeof(unsigned));
+constexpr size_t kNaCtl = kNaHeavy + 256;
+constexpr size_t kNaBad = kNaCtl + kNoAllocAlign(sizeof(Ctl));
+constexpr size_t kNoAllocBytes = kNaBad + 256;
+
+}  // namespace i2
+
+// The scratch itself. In host code this name is only a host-side stand-in:
+// its device address is obtained with cudaGetSymbolAddress (per device).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[i2::kNoAllocBytes];
+
+namespace i2 {
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_dev[64] = {nullptr};
+
+// Device address of the scratch on the current device; looked up on the first
+// call per device.
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  I2_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return I2_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_dev[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return cuda_status(e);
+    }
+    g_noalloc_dev[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_dev[dev];
+  return I2_OK;
+}
+
+}  // namespace i2
+
+extern "C" int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* dist_dev, void* stream,
+                              int* iterations) {
+  using namespace i2;
+  if (algo < I2_BFS || algo > I2_CC || !dev || !dist_dev) return I2_ERR_ARG;
+  if (dev->nodes < 1 || dev->edges < 0 || !dev->nindex || (dev->edges > 0 && !dev->nlist)) return I2_ERR_ARG;
+  if (dev->nodes > kNoAllocMaxNodes) return I2_ERR_CAPACITY;
+  if (algo != I2_CC && (src < 0 || src >= dev->nodes)) return I2_ERR_ARG;
+  if (algo == I2_SSSP && !dev->eweight) return I2_ERR_ARG;
+  if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
+  const int* w = algo == I2_SSSP ? dev->eweight : nullptr;
+  if (!device_range_ok(dev->nindex, sizeof(int) * ((size_t)dev->nodes + 1)) ||
+      !device_range_ok(dev->nlist, sizeof(int) * (size_t)dev->edges) ||
+      (w && !device_range_ok(w, sizeof(int) * (size_t)dev->edges)) ||
+      !device_range_ok(dist_dev, sizeof(int) * (size_t)dev->nodes))
+    return I2_ERR_ARG;
+  unsigned char* base = nullptr;
+  int st = noalloc_scratch(&base);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctl* ctl = reinterpret_cast<Ctl*>(base + kNaCtl);
+  int* bad = reinterpret_cast<int*>(base + kNaBad);
+
+  Ctx c{};
+  c.g.nodes = dev->nodes;
+  c.g.edges = dev->edges;
+  c.g.nindex = dev->nindex;
+  c.g.nlist = dev->nlist;
+  c.g.eweight = w;
+  c.g.sp = nullptr;
+  c.g.vec_ok = ((((uintptr_t)dev->nlist) & 15) == 0 && (((uintptr_t)w) & 15) == 0) ? 1 : 0;
+  c.gs.nodes = dev->nodes;
+  c.gs.edges = dev->edges;
+  c.gs.wmin = 1;
+  c.gs.avgdeg = (float)dev->edges / (float)dev->nodes;
+  c.dist = dist_dev;
+  for (int k = 0; k < 3; ++k) {
+    c.wl[k] = reinterpret_cast<int*>(base + kNaWl) + (size_t)k * kNoAllocMaxNodes;
+    c.woff[k] = reinterpret_cast<unsigned*>(base + kNaWoff) + (size_t)k * kNoAllocMaxNodes;
+    c.bm[k] = reinterpret_cast<unsigned*>(base + kNaBm) + (size_t)k * kNoAllocWords;
+    // the heavy lists stay empty: the threshold is above every degree
+    c.hwl[k] = reinterpret_cast<int*>(base + kNaHeavy);
+    c.htoff[k] = reinterpret_cast<unsigned*>(base + kNaHeavy + 128);
+  }
+  c.ctl = ctl;
+  c.recs = nullptr;
+  c.rec_cap = 0;
+  c.heavy = INT_MAX;
+  c.bm_words = (dev->nodes + 31) / 32;
+  c.mlp = nullptr;
+  c.srcs = nullptr;
+  c.use_loop = 0;
+  c.use_switch = 0;
+
+  // Reject malformed arrays before any traversal kernel indexes through them.
+  int hbad = 0;
+  I2_CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  k_validate<<<4 * sm_count(), 256, 0, s>>>(c.g, bad);
+  I2_CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  I2_CK(cudaStreamSynchronize(s));
+  if (hbad) return I2_ERR_FORMAT;
+
+  // The scratch keeps the previous call's contents: the bitmaps must start at
+  // zero (k_reset rewrites the control block, k_fill the output).
+  RunParams rp;
+  rp.algo = algo;
+  rp.mode = 0;
+  rp.fixed_variant = kVPCta;
+  rp.allowed = 1 << kVPCta;
+  rp.src = algo == I2_CC ? 0 : src;
+  rp.nsrc = 1;
+  rp.iter_cap = dev->nodes + 2;
+  I2_CK(cudaMemsetAsync(c.bm[0], 0, sizeof(unsigned) * 3ull * kNoAllocWords, s));
+  k_reset<<<1, 32, 0, s>>>(ctl, rp);
+  KernelFn ff = fill_kernel(algo);
+  ff<<<grid_for(ff, 8), kBlock, 0, s>>>(c);
+  seed_kernel(algo)<<<1, kBlock, 0, s>>>(c);
+  KernelFn fn = relax_kernel(algo, kVPCta);
+  const int grid = grid_for(fn, 8);
+  Ctl h;
+  for (;;) {
+    I2_CK(cudaMemcpyAsync(&h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    I2_CK(cudaStreamSynchronize(s));
+    if (slot_size(h.slot[h.iter % 3].packed) == 0 || (h.status & kStatusIterCap)) break;
+    fn<<<grid, kBlock, 0, s>>>(c);
+    I2_CK(cudaGetLastError());
+  }
+  if (iterations) *iterations = h.iter;
+  return (h.status & kStatusIterCap) ? I2_ERR_ITER_CAP : I2_OK;
+}
