@@ -231,9 +231,11 @@ def run_ours(args, rank: int, world: int, local: int):
     if cert is not None:
         raise SystemExit(f"result certificate failed: {cert}")
 
+    loop = i2.I2_LOOP_HOST if args.loop == "host" else i2.I2_LOOP_GRAPH
+
     def steps(n, v=variant):
         for _ in range(n):
-            dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, report=False)
+            dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, loop=loop, report=loop == i2.I2_LOOP_HOST)
 
     with torch.cuda.stream(stream):
         steps(args.warmup)
@@ -278,7 +280,7 @@ def run_ours(args, rank: int, world: int, local: int):
     if SELECTOR_PARAMS.exists():
         i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
         cand.append("learned")
-    for v in cand:
+    for v in ([] if args.no_styles else cand):
         name = v if isinstance(v, str) else i2.VARIANTS[v]
         if v in (4, 5) and not dg.info["symmetric"]:
             continue
@@ -291,7 +293,7 @@ def run_ours(args, rank: int, world: int, local: int):
         f1.record(stream)
         f1.synchronize()
         styles[name] = 1e-9 * E / (f0.elapsed_time(f1) / args.style_steps * 1e-3)
-    fixed = {k: v for k, v in styles.items() if k not in ("heuristic", "learned")}
+    fixed = {k: v for k, v in styles.items() if k not in ("heuristic", "learned")} or {variant: value / world}
 
     # end to end through the C ABI from pinned host buffers
     hp = i2.ECLGraph(V, E, pinned_copy(host.nindex), pinned_copy(host.nlist), pinned_copy(host.eweight))
@@ -334,7 +336,8 @@ def run_ours(args, rank: int, world: int, local: int):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}"),
+            "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}",
+                           loop=args.loop),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_query": e2e_query,
             "gpu_launches": launches, "clocks": clk,
             "styles_gteps": styles, "best_fixed_style": max(fixed, key=fixed.get),
@@ -356,6 +359,10 @@ def main():
     ap.add_argument("--style-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-styles", action="store_true", help="skip the per-style comparison")
+    ap.add_argument("--loop", choices=["graph", "host"], default="graph",
+                    help="device loop in one CUDA graph (default) or one host launch per iteration "
+                         "(for per-kernel profiling)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if world != args.gpus and not (world == 1 and args.gpus == 1):

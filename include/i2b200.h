@@ -183,8 +183,10 @@ int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* o
 int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n);
 
 /* Per-iteration sweep for selector training: follows the trajectory of `follow`
-   and times every allowed variant from each iteration's state (state saved and
-   restored on the device). times[it * I2_NUM_VARIANTS + v] in ns (-1: not allowed). */
+   (a variant, I2_AUTO_HEURISTIC or I2_AUTO_LEARNED) and times every allowed
+   variant from each iteration's state (state saved and restored on the device,
+   each launch bracketed by CUDA events, best of `reps`).
+   times[it * I2_NUM_VARIANTS + v] in ns (-1: not allowed). */
 int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_record* recs,
              float* times, int cap, int* n);
 

@@ -109,7 +109,9 @@ struct Ctl {
   int src;                  // source vertex (BFS/SSSP)
   int nsrc;                 // number of sources (batched runs)
   int algo;
-  int pad[2];
+  int sel_n;                // frontier entries at the last selector evaluation
+  unsigned sel_e;           // frontier edges at the last selector evaluation
+  int sel_iter;             // iteration of the last selector evaluation
   unsigned long long relax_ns;  // sum of relax launch durations
   float feat[kFeatures];    // features of the frontier the next launch consumes
 };
@@ -151,9 +153,7 @@ struct Ctx {
   const float* mlp;         // selector weights (device), may be null
   const int* srcs;          // batched sources (device), may be null
   unsigned long long loop_h;   // cudaGraphConditionalHandle of the while node
-  unsigned long long switch_h; // cudaGraphConditionalHandle of the switch node
   int use_loop;
-  int use_switch;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {

@@ -6,8 +6,9 @@
 // empty (the do-while of the reference's host drivers, e.g.
 // BFS_CUDA_V_Data_Push_..._Warp_..._NonDup.cu:112-122). In the default loop
 // mode the whole sequence is one CUDA graph: a WHILE conditional node whose
-// body is either the fixed variant's relax kernel or a SWITCH node over all
-// variants. The relax kernels' last block decides both conditions on the
+// body is one kernel, either the fixed style's relax kernel or the dispatch
+// kernel whose blocks branch on the style picked for this iteration. The relax
+// kernels' last block picks the next style and sets the loop condition on the
 // device, so there is no host round trip per iteration.
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -46,21 +47,32 @@ __device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size,
 }
 
 // Executed by every thread of one block. Computes the features of the frontier
-// in slot `nxt`, picks the variant for the next launch and sets the graph's
-// switch condition. `cond` tells whether another launch will happen.
+// in slot `nxt`, picks the variant for the next launch and sets the loop
+// condition of the graph. `cond` tells whether another launch will happen.
+// The learned selector is re-evaluated when the frontier's entries or edges
+// moved by more than a factor 1.5 since its last evaluation, or 16 iterations
+// passed; otherwise the previous choice stands (long tails of small, similar
+// frontiers do not pay for an inference each).
 __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], y[kOut];
+  __shared__ int s_eval;
   Ctl* ctl = c.ctl;
   if (threadIdx.x == 0) {
     volatile Slot* sl = &ctl->slot[nxt];
     const unsigned long long p = sl->packed;
-    frontier_features(c.gs, ctl->algo, next_iter, slot_size(p), slot_size(sl->hpacked), slot_edges(p), sl->maxdeg,
+    const int n = slot_size(p);
+    const unsigned e = slot_edges(p);
+    frontier_features(c.gs, ctl->algo, next_iter, n, slot_size(sl->hpacked), e, sl->maxdeg,
                       *(volatile long long*)&ctl->visited, x);
     for (int k = 0; k < kFeatures; ++k) ctl->feat[k] = x[k];
+    const long long sn = ctl->sel_n, se = ctl->sel_e;
+    s_eval = next_iter == 0 || 2LL * n > 3LL * sn || 3LL * n < 2LL * sn || 2LL * e > 3LL * se ||
+             3LL * e < 2LL * se || next_iter - ctl->sel_iter >= 16;
   }
   __syncthreads();
   const int mode = ctl->mode;
-  if (mode == 2 && c.mlp && cond) mlp_forward_block(c.mlp, x, h1, h2, y);
+  const bool infer = mode == 2 && c.mlp && cond && s_eval;
+  if (infer) mlp_forward_block(c.mlp, x, h1, h2, y);
   if (threadIdx.x == 0) {
     int v = ctl->fixed_variant;
     if (mode == 1 || (mode == 2 && !c.mlp)) {
@@ -68,18 +80,25 @@ __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
       const unsigned long long p = sl->packed;
       v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, slot_size(p), slot_edges(p));
     } else if (mode == 2) {
-      float best = 3.0e38f;
-      v = -1;
-      for (int k = 0; k < kOut; ++k)
-        if (((ctl->allowed >> k) & 1) && y[k] < best) {
-          best = y[k];
-          v = k;
-        }
-      if (v < 0) v = kVPThread;
+      v = ctl->variant;
+      if (infer) {
+        float best = 3.0e38f;
+        int bv = -1;
+        for (int k = 0; k < kOut; ++k)
+          if (((ctl->allowed >> k) & 1) && y[k] < best) {
+            best = y[k];
+            bv = k;
+          }
+        v = bv < 0 ? kVPCta : bv;
+        volatile Slot* sl = &ctl->slot[nxt];
+        const unsigned long long p = sl->packed;
+        ctl->sel_n = slot_size(p);
+        ctl->sel_e = slot_edges(p);
+        ctl->sel_iter = next_iter;
+      }
     }
     ctl->variant = v;
     if (cond) ctl->hist[v] += 1;
-    if (c.use_switch) cudaGraphSetConditional((cudaGraphConditionalHandle)c.switch_h, cond ? (unsigned)v : 0xffffu);
     if (c.use_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)c.loop_h, cond ? 1u : 0u);
   }
 }
@@ -367,6 +386,12 @@ static KernelFn relax_fn(int v) {
     case kPushTopo: return relax_push_topo<ALG>;
   }
   return nullptr;
+}
+
+static KernelFn dispatch_kernel(int algo) {
+  if (algo == kBFS) return relax_dispatch<kBFS>;
+  if (algo == kSSSP) return relax_dispatch<kSSSP>;
+  return relax_dispatch<kCC>;
 }
 
 KernelFn relax_kernel(int algo, int v) {
@@ -720,16 +745,12 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   cudaGraph_t gr;
   I2_CK(cudaGraphCreate(&gr, 0));
   g->graphs.push_back(gr);
-  cudaGraphConditionalHandle loop_h, sw_h = 0;
+  cudaGraphConditionalHandle loop_h;
   I2_CK(cudaGraphConditionalHandleCreate(&loop_h, gr, 1, cudaGraphCondAssignDefault));
-  const bool sw = mode != 0;
-  if (sw) I2_CK(cudaGraphConditionalHandleCreate(&sw_h, gr, 0, cudaGraphCondAssignDefault));
   Ctx c = make_ctx(g);
   c.srcs = multi ? g->srcs : nullptr;
   c.loop_h = (unsigned long long)loop_h;
-  c.switch_h = (unsigned long long)sw_h;
   c.use_loop = 1;
-  c.use_switch = sw ? 1 : 0;
   // bitmaps <- 0
   cudaGraphNode_t n_ms, n_reset, n_fill, n_seed, n_loop;
   cudaMemsetParams ms{};
@@ -763,25 +784,13 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   cp.conditional.size = 1;
   I2_CK(cudaGraphAddNode(&n_loop, gr, &n_seed, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  if (!sw) {
+  // The loop body is one kernel: the fixed style's, or the dispatch kernel
+  // whose blocks branch on the style the previous iteration selected.
+  {
     cudaGraphNode_t n;
-    KernelFn fn = relax_kernel(algo, variant);
+    KernelFn fn = mode == 0 ? relax_kernel(algo, variant) : dispatch_kernel(algo);
     st = add_kernel_node(body, &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
     if (st) return st;
-  } else {
-    cudaGraphNodeParams sp{};
-    sp.type = cudaGraphNodeTypeConditional;
-    sp.conditional.handle = sw_h;
-    sp.conditional.type = cudaGraphCondTypeSwitch;
-    sp.conditional.size = kNumVariants;
-    cudaGraphNode_t n_sw;
-    I2_CK(cudaGraphAddNode(&n_sw, body, nullptr, 0, &sp));
-    for (int v = 0; v < kNumVariants; ++v) {
-      cudaGraphNode_t n;
-      KernelFn fn = relax_kernel(algo, v);
-      st = add_kernel_node(sp.conditional.phGraph_out[v], &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
-      if (st) return st;
-    }
   }
   ExecEntry e;
   I2_CK(cudaGraphInstantiate(&e.ex, gr, 0));
@@ -986,7 +995,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
     I2_CK(cudaMalloc(&g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words));
   }
   cudaStream_t s = g->stream;
-  const int mode = follow < 0 ? 1 : 0;
+  const int mode = follow == I2_AUTO_LEARNED ? 2 : (follow < 0 ? 1 : 0);
   st = prepare_run(g, s, make_params(g, algo, mode, follow < 0 ? 0 : follow, src, 1, 0));
   if (st) return st;
   Ctx c = make_ctx(g);
@@ -1004,18 +1013,20 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
     if (slot_size(snap.slot[cur].packed) == 0) break;
     I2_CK(cudaMemcpyAsync(g->snap_dist, g->dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
     I2_CK(cudaMemcpyAsync(g->snap_bm, g->bm[0], sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
+    // Styles are timed through the dispatch kernel, the one the selectors run.
+    KernelFn dk = dispatch_kernel(algo);
+    const int dgrid = grid_for(dk, g->blocks_per_sm);
     for (int v = 0; v < kNumVariants; ++v) {
       float best = -1.f;
       if ((allowed >> v) & 1) {
-        KernelFn fn = relax_kernel(algo, v);
-        const int grid = grid_for(fn, g->blocks_per_sm);
         for (int r = 0; r < std::max(1, reps); ++r) {
           *g->h_ctl = snap;
+          g->h_ctl->variant = v;
           I2_CK(cudaMemcpyAsync(g->ctl, g->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
           I2_CK(cudaMemcpyAsync(g->dist, g->snap_dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
           I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
           I2_CK(cudaEventRecord(g->ev0, s));
-          fn<<<grid, kBlock, 0, s>>>(c);
+          dk<<<dgrid, kBlock, 0, s>>>(c);
           I2_CK(cudaEventRecord(g->ev1, s));
           I2_CK(cudaEventSynchronize(g->ev1));
           float ms = 0.f;
@@ -1030,8 +1041,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
     I2_CK(cudaMemcpyAsync(g->ctl, g->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
     I2_CK(cudaMemcpyAsync(g->dist, g->snap_dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
     I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
-    KernelFn fn = relax_kernel(algo, snap.variant);
-    fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
+    dk<<<dgrid, kBlock, 0, s>>>(c);
     I2_CK(cudaGetLastError());
     if (snap.iter < g->rec_cap)
       I2_CK(cudaMemcpyAsync(&recs[it], g->recs + snap.iter, sizeof(IterRec), cudaMemcpyDeviceToHost, s));
@@ -1343,7 +1353,7 @@ int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n) {
 int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_record* recs, float* times, int cap,
              int* n) {
   if (!g || !recs || !times || !n || cap < 1 || algo < I2_BFS || algo > I2_CC) return I2_ERR_ARG;
-  if (follow >= kNumVariants) return I2_ERR_ARG;
+  if (follow >= kNumVariants || follow < I2_AUTO_LEARNED) return I2_ERR_ARG;
   if (algo != I2_CC && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
   if (algo == I2_SSSP && !g->g.eweight) return I2_ERR_ARG;
   if (follow >= 0) {
@@ -1474,7 +1484,6 @@ extern "C" int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* di
   c.mlp = nullptr;
   c.srcs = nullptr;
   c.use_loop = 0;
-  c.use_switch = 0;
 
   // Reject malformed arrays before any traversal kernel indexes through them.
   int hbad = 0;

@@ -10,6 +10,8 @@
 
 namespace i2 {
 
+static_assert(kBlock == 4 * 64 && kNumVariants * 32 <= kBlock, "mlp_forward_block assumes 256 threads");
+
 constexpr int kOut = kNumVariants;
 constexpr int kOffMu = 0;
 constexpr int kOffSd = kOffMu + kFeatures;
@@ -47,33 +49,52 @@ __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, in
   f[15] = fs > 0.f ? (float)hsize / fs : 0.f;
 }
 
-// Block-cooperative forward pass (any block size >= kHidden). x and y live in
-// shared memory; the hidden activations use the two scratch arrays.
+// Block-cooperative forward pass for a block of kBlock (256) threads. Each
+// hidden unit is computed by 4 threads (partial dot products reduced with
+// shuffles) and each output by one warp, so every thread issues at most 16
+// independent weight loads per layer instead of a chain of 64. x and y live in
+// shared memory; h1 and h2 are shared scratch.
 __device__ __forceinline__ void mlp_forward_block(const float* __restrict__ P, const float* x, float* h1,
                                                   float* h2, float* y) {
   const int t = threadIdx.x;
-  if (t < kHidden) {
-    float acc = P[kOffB1 + t];
+  const int j = t >> 2;  // hidden unit
+  const int q = t & 3;   // quarter of its inputs
+  if (t < 4 * kHidden) {
+    float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < kFeatures; ++k) {
+    for (int i = 0; i < kFeatures / 4; ++i) {
+      const int k = q * (kFeatures / 4) + i;
       const float xs = (x[k] - P[kOffMu + k]) / P[kOffSd + k];
-      acc = fmaf(xs, P[kOffW1 + k * kHidden + t], acc);
+      acc = fmaf(xs, P[kOffW1 + k * kHidden + j], acc);
     }
-    h1[t] = fmaxf(acc, 0.f);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (q == 0) h1[j] = fmaxf(acc + P[kOffB1 + j], 0.f);
   }
   __syncthreads();
-  if (t < kHidden) {
-    float acc = P[kOffB2 + t];
-#pragma unroll 8
-    for (int k = 0; k < kHidden; ++k) acc = fmaf(h1[k], P[kOffW2 + k * kHidden + t], acc);
-    h2[t] = fmaxf(acc, 0.f);
+  if (t < 4 * kHidden) {
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < kHidden / 4; ++i) {
+      const int k = q * (kHidden / 4) + i;
+      acc = fmaf(h1[k], P[kOffW2 + k * kHidden + j], acc);
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (q == 0) h2[j] = fmaxf(acc + P[kOffB2 + j], 0.f);
   }
   __syncthreads();
-  if (t < kOut) {
-    float acc = P[kOffB3 + t];
-#pragma unroll 8
-    for (int k = 0; k < kHidden; ++k) acc = fmaf(h2[k], P[kOffW3 + k * kOut + t], acc);
-    y[t] = acc;
+  const int o = t >> 5;  // output of this warp
+  const int lane = t & 31;
+  if (o < kOut) {
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < kHidden / 32; ++i) {
+      const int k = lane * (kHidden / 32) + i;
+      acc = fmaf(h2[k], P[kOffW3 + k * kOut + o], acc);
+    }
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    if (lane == 0) y[o] = acc + P[kOffB3 + o];
   }
   __syncthreads();
 }

@@ -353,23 +353,23 @@ __device__ __forceinline__ void stage_flush_if_half(const Ctx& c, Stage& s, int 
   if (full) stage_flush(c, s, nxt);
 }
 
-// Contiguous share [lo, hi) of [0, total) for this block.
-__device__ __forceinline__ void block_share(unsigned total, unsigned* lo, unsigned* hi) {
-  *lo = (unsigned)(((unsigned long long)total * blockIdx.x) / gridDim.x);
-  *hi = (unsigned)(((unsigned long long)total * (blockIdx.x + 1)) / gridDim.x);
+// Contiguous share [lo, hi) of [0, total) for this block among `nb` blocks.
+__device__ __forceinline__ void block_share(unsigned total, int nb, unsigned* lo, unsigned* hi) {
+  *lo = (unsigned)(((unsigned long long)total * blockIdx.x) / nb);
+  *hi = (unsigned)(((unsigned long long)total * (blockIdx.x + 1)) / nb);
 }
 
 // Heavy frontier vertices: their adjacency is cut into tiles of kHeavyTile
 // entries. Each block takes a contiguous share of the tile sequence, finds the
 // vertex of its first tile once, and walks forward.
 template <int ALG>
-__device__ void heavy_path(const Ctx& c, Stage& s, Acc& a, int cur, int nxt) {
+__device__ void heavy_path(const Ctx& c, Stage& s, Acc& a, int cur, int nxt, int active) {
   const unsigned long long hp = c.ctl->slot[cur].hpacked;
   const int nh = slot_size(hp);
   const unsigned ntiles = slot_edges(hp);
   if (ntiles == 0) return;
   unsigned t0, t1;
-  block_share(ntiles, &t0, &t1);
+  block_share(ntiles, active, &t0, &t1);
   if (t0 >= t1) return;  // uniform
   const unsigned* __restrict__ toff = c.htoff[cur];
   if (threadIdx.x < 32) {
@@ -391,12 +391,13 @@ __device__ void heavy_path(const Ctx& c, Stage& s, Acc& a, int cur, int nxt) {
   }
 }
 
-// Clear the bitmap of F_{i-1} (slot old): by entries when it is small, by words otherwise.
-__device__ __forceinline__ void clear_old(const Ctx& c, int old) {
+// Clear the bitmap of F_{i-1} (slot old): by entries when it is small, by
+// words otherwise. Spread over the launch's `active` blocks.
+__device__ __forceinline__ void clear_old(const Ctx& c, int old, int active) {
   const int n = slot_size(c.ctl->slot[old].packed);
   unsigned* bm = c.bm[old];
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long stride = (long long)active * blockDim.x;
   if ((long long)n * 4 > c.bm_words) {
     for (long long w = tid; w < c.bm_words; w += stride) bm[w] = 0u;
   } else {
@@ -407,9 +408,25 @@ __device__ __forceinline__ void clear_old(const Ctx& c, int old) {
 
 __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old);
 
-// Common epilogue: publish block statistics and let the last block finish the iteration.
+// Blocks of a launch that take part in it. Blocks at or above this index
+// return at once, so a small frontier does not pay for the whole grid; the
+// clearing of F_{i-1} is work too. Full sweeps pass `need` = gridDim.x.
+__device__ __forceinline__ int active_blocks(const Ctx& c, int old, long long need) {
+  const int n_old = slot_size(c.ctl->slot[old].packed);
+  const long long clear = ((long long)n_old * 4 > c.bm_words) ? ((long long)c.bm_words + 8191) / 8192
+                                                                : ((long long)n_old + 2047) / 2048;
+  long long a = need > clear ? need : clear;
+  if (a < 1) a = 1;
+  if (a > gridDim.x) a = gridDim.x;
+  return (int)a;
+}
+
+// Common epilogue: publish block statistics and let the last block finish the
+// iteration. Every block of the launch, active or not, counts into `done`, so
+// the iteration advances only after every block has read its state.
 template <typename S>
-__device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a, int i, int cur, int nxt, int old) {
+__device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a, int i, int cur, int nxt, int old,
+                                               int /*active*/) {
   acc_reduce(a, s);
   if (threadIdx.x == 0) {
     const Acc& r = s.red[0];
@@ -428,8 +445,25 @@ __device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a,
   }
 }
 
+// The launch's start time is taken by block 0, which the scheduler dispatches
+// first; the last block reads it after every block has finished.
+// Epilogue of a block with no work in this launch.
+template <typename S>
+__device__ __forceinline__ void idle_epilogue(const Ctx& c, S& s, int i, int cur, int nxt, int old) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(&c.ctl->done, 1u);
+    s.last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s.last) {
+    __threadfence();
+    finish_iteration(c, i, cur, nxt, old);
+  }
+}
+
 __device__ __forceinline__ void block_prologue(const Ctx& c) {
-  if (threadIdx.x == 0) atomicMin(&c.ctl->tstart, globaltimer());
+  if (blockIdx.x == 0 && threadIdx.x == 0) c.ctl->tstart = globaltimer();
 }
 
 // ---------------------------------------------------------------------------
@@ -437,20 +471,23 @@ __device__ __forceinline__ void block_prologue(const Ctx& c) {
 // vertex. Heavy vertices are skipped here and taken by the heavy path.
 
 template <int ALG, int VAR>
-__global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
-  __shared__ Stage s;
+__device__ __forceinline__ void body_push(const Ctx& c, Stage& s) {
   block_prologue(c);
+  const int i = c.ctl->iter;
+  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
+  const int n = slot_size(c.ctl->slot[cur].packed);
+  const int per = VAR == kVPThread ? kBlock : (VAR == kVPWarp ? kBlock / kWarp : 1);
+  const int active = active_blocks(c, old, ((long long)n + per - 1) / per + slot_edges(c.ctl->slot[cur].hpacked));
+  if (blockIdx.x >= active) {
+    idle_epilogue(c, s, i, cur, nxt, old);
+    return;
+  }
   stage_init(s);
   Acc a;
   acc_init(a);
-  const int i = c.ctl->iter;
-  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  clear_old(c, old);
+  clear_old(c, old, active);
   __syncthreads();
-
-  const int n = slot_size(c.ctl->slot[cur].packed);
   const int* __restrict__ wl = c.wl[cur];
-  const int per = VAR == kVPThread ? kBlock : (VAR == kVPWarp ? kBlock / kWarp : 1);
 
   for (;;) {
     if (threadIdx.x == 0) s.chunk = atomicAdd(&c.ctl->chunk, per);
@@ -483,9 +520,9 @@ __global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
     }
     stage_flush_if_half(c, s, nxt);
   }
-  heavy_path<ALG>(c, s, a, cur, nxt);
+  heavy_path<ALG>(c, s, a, cur, nxt, active);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -611,33 +648,47 @@ struct EpiStage {
 #define I2_EB_MIN_BLOCKS 6
 #endif
 
+struct EBShared {
+  EpiStage s;
+  WarpStage wss[kWarpsPerBlock];
+};
+
 template <int ALG>
-__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(Ctx c) {
-  __shared__ EpiStage s;
-  __shared__ WarpStage wss[kWarpsPerBlock];
+__device__ __forceinline__ void body_edge_balanced(const Ctx& c, EBShared& sh) {
+  EpiStage& s = sh.s;
   block_prologue(c);
-  if (threadIdx.x == 0) s.last = 0;
-  Acc a;
-  acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  clear_old(c, old);
-  const int lane = threadIdx.x & 31;
-  WarpStage& ws = wss[threadIdx.x >> 5];
-  if (lane == 0) ws.n = 0;
-  __syncwarp();
-
   const unsigned long long P = c.ctl->slot[cur].packed;
   const int n = slot_size(P);
   const unsigned total = slot_edges(P);
+  const int active = active_blocks(c, old, ((long long)total + kWarpTile * kWarpsPerBlock - 1) /
+                                              (kWarpTile * kWarpsPerBlock));
+  if (blockIdx.x >= active) {
+    idle_epilogue(c, s, i, cur, nxt, old);
+    return;
+  }
+  if (threadIdx.x == 0) s.last = 0;
+  Acc a;
+  acc_init(a);
+  clear_old(c, old, active);
+  const int lane = threadIdx.x & 31;
+  WarpStage& ws = sh.wss[threadIdx.x >> 5];
+  if (lane == 0) ws.n = 0;
+  __syncwarp();
   const int* __restrict__ wl = c.wl[cur];
   const unsigned* __restrict__ woff = c.woff[cur];
   const int* __restrict__ nl = c.g.nlist;
   const int* __restrict__ ew = c.g.eweight;
+  // Only as many warps as there are warp tiles take part, so a small frontier
+  // is not spread over (and searched by) every warp of the grid.
   const unsigned long long gw = (unsigned long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  const unsigned long long nw = (unsigned long long)gridDim.x * kWarpsPerBlock;
-  const unsigned W0 = (unsigned)((total * gw) / nw);
-  const unsigned W1 = (unsigned)((total * (gw + 1)) / nw);
+  const unsigned long long need = ((unsigned long long)total + kWarpTile - 1) / kWarpTile;
+  const unsigned long long nw = need < (unsigned long long)active * kWarpsPerBlock
+                                    ? (need > 0 ? need : 1)
+                                    : (unsigned long long)active * kWarpsPerBlock;
+  const unsigned W0 = gw < nw ? (unsigned)((total * gw) / nw) : 0u;
+  const unsigned W1 = gw < nw ? (unsigned)((total * (gw + 1)) / nw) : 0u;
   if (W0 < W1) {
     int j = owner_search_warp(woff, n, W0);  // entry holding edge W0
     for (unsigned e0 = W0; e0 < W1; e0 += kWarpTile) {
@@ -687,22 +738,22 @@ __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(
   }
   warp_flush(c, ws, nxt);
   __syncthreads();
-  block_epilogue(c, s, a, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
 // Bitmap-gated topology sweep: thread per vertex, light vertices only; heavy
 // frontier vertices take the shared heavy path.
 template <int ALG>
-__global__ void __launch_bounds__(kBlock) relax_push_topo(Ctx c) {
-  __shared__ Stage s;
+__device__ __forceinline__ void body_push_topo(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
   acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  clear_old(c, old);
+  const int active = gridDim.x;  // topology sweeps use the whole grid
+  clear_old(c, old, active);
   __syncthreads();
   const unsigned* __restrict__ bmc = c.bm[cur];
   const int V = c.g.nodes;
@@ -716,23 +767,23 @@ __global__ void __launch_bounds__(kBlock) relax_push_topo(Ctx c) {
     }
     stage_flush_if_half(c, s, nxt);
   }
-  heavy_path<ALG>(c, s, a, cur, nxt);
+  heavy_path<ALG>(c, s, a, cur, nxt, active);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
 // Edge-centric sweep over all CSR entries, gated by the source's frontier bit.
 template <int ALG>
-__global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
-  __shared__ Stage s;
+__device__ __forceinline__ void body_edge_topo(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
   acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  clear_old(c, old);
+  const int active = gridDim.x;  // topology sweeps use the whole grid
+  clear_old(c, old, active);
   __syncthreads();
   const unsigned* __restrict__ bmc = c.bm[cur];
   const int E = c.g.edges;
@@ -777,7 +828,7 @@ __global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
     stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -786,15 +837,15 @@ __global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
 // frontier's bitmap is written with one plain store per warp. dist[v] is only
 // written by v's own thread, so no atomics are needed on it.
 template <int ALG, bool FRONTIER>
-__global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
-  __shared__ Stage s;
+__device__ __forceinline__ void body_pull(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
   acc_init(a);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  clear_old(c, old);
+  const int active = gridDim.x;  // every vertex is visited
+  clear_old(c, old, active);
   __syncthreads();
   const unsigned* __restrict__ bmc = c.bm[cur];
   const int V = c.g.nodes;
@@ -842,7 +893,63 @@ __global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
     stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old);
+  block_epilogue(c, s, a, i, cur, nxt, old, active);
+}
+
+// ---------------------------------------------------------------------------
+// Kernels: one per (algorithm, style) for fixed-style runs, and one dispatch
+// kernel per algorithm for the selectors, whose blocks branch on the style
+// chosen at the end of the previous iteration (one kernel node per iteration
+// instead of a conditional SWITCH node).
+
+template <int ALG, int VAR>
+__global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
+  __shared__ Stage s;
+  body_push<ALG, VAR>(c, s);
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(Ctx c) {
+  __shared__ EBShared sh;
+  body_edge_balanced<ALG>(c, sh);
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock) relax_push_topo(Ctx c) {
+  __shared__ Stage s;
+  body_push_topo<ALG>(c, s);
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
+  __shared__ Stage s;
+  body_edge_topo<ALG>(c, s);
+}
+
+template <int ALG, bool FRONTIER>
+__global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
+  __shared__ Stage s;
+  body_pull<ALG, FRONTIER>(c, s);
+}
+
+union AnyShared {
+  Stage st;
+  EBShared eb;
+};
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_dispatch(Ctx c) {
+  __shared__ AnyShared sh;
+  switch (c.ctl->variant) {  // same value for every thread of the launch
+    case kVPThread: body_push<ALG, kVPThread>(c, sh.st); break;
+    case kVPWarp: body_push<ALG, kVPWarp>(c, sh.st); break;
+    case kVPCta: body_edge_balanced<ALG>(c, sh.eb); break;
+    case kVPBlock: body_push<ALG, kVPBlock>(c, sh.st); break;
+    case kPullFrontier: body_pull<ALG, true>(c, sh.st); break;
+    case kPullTopo: body_pull<ALG, false>(c, sh.st); break;
+    case kEdgeTopo: body_edge_topo<ALG>(c, sh.st); break;
+    default: body_push_topo<ALG>(c, sh.st); break;
+  }
 }
 
 }  // namespace i2

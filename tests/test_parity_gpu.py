@@ -9,7 +9,15 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 FIXED = list(range(i2.I2_NUM_VARIANTS))
-ALL = FIXED + ["heuristic"]
+ALL = FIXED + ["heuristic", "learned"]
+
+
+@pytest.fixture(autouse=True, scope="module")
+def _selector_params():
+    from indigo2suite_b200 import selector
+
+    if i2.device_count() > 0:
+        i2.mlp_set_params(np.fromfile(selector.PARAMS_PATH, np.float32))
 
 
 def _variants_for(dg):

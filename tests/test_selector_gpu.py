@@ -1,0 +1,51 @@
+"""The learned style selector (committed parameters) on graphs it was not
+trained on: it never changes a result, and it is faster than the fixed
+frontier-size heuristic it replaces."""
+import math
+
+import numpy as np
+import pytest
+
+import indigo2suite_b200 as i2
+import oracle
+from indigo2suite_b200 import selector as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def params(gpu):
+    p = np.fromfile(S.PARAMS_PATH, np.float32)
+    assert p.size == i2.mlp_param_count()
+    i2.mlp_set_params(p)
+    return p
+
+
+def _median_ms(dg, algo, src, variant, runs=5):
+    dg.run_device(algo, src, variant=variant)
+    return sorted(dg.run_device(algo, src, variant=variant).seconds for _ in range(runs))[runs // 2] * 1e3
+
+
+def test_learned_results_are_bit_exact(params):
+    for g in (i2.gen_rmat(16, 16, seed=901), i2.gen_grid(160, 0.05, 0.001, 902), i2.gen_er(30000, 120000, 903)):
+        dg = i2.DeviceGraph.upload(g)
+        src = int(np.argmax(g.degrees()))
+        d, rep = dg.bfs(src, variant="learned")
+        np.testing.assert_array_equal(d, oracle.bfs(g, src))
+        assert sum(rep.variant_hist) == rep.iterations
+        np.testing.assert_array_equal(dg.sssp(src, variant="learned")[0], oracle.sssp(g, src))
+        np.testing.assert_array_equal(dg.cc(variant="learned")[0], oracle.cc(g))
+        dg.free()
+
+
+def test_learned_beats_the_fixed_heuristic_on_held_out_graphs(params):
+    ratios = []
+    for spec in (S.GraphSpec("er", 19, 8101), S.GraphSpec("grid", 19, 8102), S.GraphSpec("rmat", 19, 8103)):
+        g = spec.build()
+        dg = i2.DeviceGraph.upload(g)
+        src = int(np.argmax(g.degrees()))
+        for algo in (i2.I2_CC, i2.I2_SSSP):
+            ratios.append(_median_ms(dg, algo, src, "learned") / _median_ms(dg, algo, src, "heuristic"))
+        dg.free()
+    geo = math.exp(sum(math.log(r) for r in ratios) / len(ratios))
+    assert geo < 0.95, ratios
