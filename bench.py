@@ -349,6 +349,189 @@ def run_ours(args, rank: int, world: int, local: int):
     dist.close()
 
 
+def _event_time(torch, stream, fn, steps: int) -> float:
+    """Device seconds per step of fn() on `stream` (CUDA events)."""
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / steps
+
+
+def run_batch512(args, rank: int, world: int, local: int):
+    """Config: 512 graphs (log-uniform 1e3..1e6 vertices, ER/RMAT/grid), BFS +
+    SSSP from each graph's highest-degree vertex; batched (one device loop for
+    all graphs) vs one launch sequence per graph. Graphs shard across ranks."""
+    import torch
+
+    import indigo2suite_b200 as i2
+    from indigo2suite_b200 import shard, workloads
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    specs = workloads.batch_specs(512)
+    lo, hi = shard.shard_range(len(specs), rank, world)
+    t0 = time.time()
+    graphs = [workloads.build(x) for x in specs[lo:hi]]
+    gen_s = time.time() - t0
+    srcs = [workloads.source(g) for g in graphs]
+    E = sum(g.edges for g in graphs)
+    V = sum(g.nodes for g in graphs)
+    b = i2.Batch(graphs)
+    per = [i2.DeviceGraph.upload(g) for g in graphs]
+    variant = args.variant
+    # parity: batched == per-graph, for both algorithms
+    for algo in (i2.I2_BFS, i2.I2_SSSP):
+        b.run_device(algo, srcs, variant=variant)
+        got = b.result()
+        for k in range(0, len(graphs), 37):
+            d, _ = per[k]._run(algo, srcs[k], variant, i2.I2_LOOP_GRAPH, 0, False, None, None)
+            if not np.array_equal(d, got[k]):
+                raise SystemExit(f"batched result differs from per-graph result (graph {k}, algo {algo})")
+
+    def batched():
+        for algo in (i2.I2_BFS, i2.I2_SSSP):
+            b.run_device(algo, srcs, variant=variant, stream=sp, report=False)
+
+    def per_graph():
+        for k, g in enumerate(per):
+            for algo in (i2.I2_BFS, i2.I2_SSSP):
+                g.run_device(algo, srcs[k], variant=variant, stream=sp, report=False)
+
+    for _ in range(args.warmup):
+        batched()
+        per_graph()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    t_b = _event_time(torch, stream, batched, args.steps)
+    clk = clocks.stop()
+    t_p = _event_time(torch, stream, per_graph, max(1, args.steps // 3))
+    # reference-shaped per-graph runs: host loop with one read-back per iteration
+    def per_graph_host():
+        for k, g in enumerate(per):
+            for algo in (i2.I2_BFS, i2.I2_SSSP):
+                g.run_device(algo, srcs[k], variant=variant, stream=sp, loop=i2.I2_LOOP_HOST)
+    t_h = _event_time(torch, stream, per_graph_host, 1)
+    t_b = dist.max(t_b, dev)
+    t_p = dist.max(t_p, dev)
+    t_h = dist.max(t_h, dev)
+    Etot = int(dist.max(float(E), dev)) if world == 1 else E
+    value = world * 2 * 1e-9 * E / t_b  # weak per-rank shares are equal in count
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_b, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "batch512_bfs_sssp", "graphs": len(specs), "graphs_this_rank": len(graphs),
+                       "nodes_this_rank": V, "edges_this_rank": E, "variant": variant,
+                       "families": "ER(avg deg 8)/RMAT(ef16)/grid, n log-uniform [1e3,1e6]",
+                       "parallelism": f"graphs sharded x{world}", "generation_s": gen_s},
+            "batched_ms": 1e3 * t_b, "per_graph_ms": 1e3 * t_p, "per_graph_host_loop_ms": 1e3 * t_h,
+            "speedup_vs_per_graph": t_p / t_b, "speedup_vs_per_graph_host_loop": t_h / t_b,
+            "clocks": clk, "verified": "batched == per-graph on every 37th graph"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.free()
+    for g in per:
+        g.free()
+    dist.close()
+
+
+def run_grid4096(args, rank: int, world: int, local: int):
+    """Config: BFS and CC on the 4096 x 4096 grid (5% removed, 0.1% long-range),
+    every fixed style, the heuristic and the learned selector."""
+    import torch
+
+    import indigo2suite_b200 as i2
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    g = i2.gen_grid(4096, 0.05, 0.001, seed=3)
+    dg = i2.DeviceGraph.upload(g)
+    if SELECTOR_PARAMS.exists():
+        i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
+    out = {}
+    for an, algo in (("bfs", i2.I2_BFS), ("cc", i2.I2_CC)):
+        res = {}
+        for v in list(range(i2.I2_NUM_VARIANTS)) + ["heuristic", "learned"]:
+            name = v if isinstance(v, str) else i2.VARIANTS[v]
+            run = lambda: dg.run_device(algo, 0, variant=v, stream=sp, report=False)  # noqa: E731
+            run()
+            torch.cuda.synchronize()
+            res[name] = 1e3 * _event_time(torch, stream, run, max(1, args.steps // 5))
+        rep = dg.run_device(algo, 0, variant="learned")
+        fixed = {k: t for k, t in res.items() if k not in ("heuristic", "learned")}
+        best = min(fixed, key=fixed.get)
+        out[an] = {"ms": res, "best_fixed": best, "learned_vs_best_fixed": fixed[best] / res["learned"],
+                   "learned_vs_heuristic": res["heuristic"] / res["learned"], "iterations_learned": rep.iterations,
+                   "variant_hist_learned": rep.variant_hist, "gteps_learned": 1e-9 * g.edges / (res["learned"] * 1e-3)}
+    line = {"metric": METRIC, "value": out["bfs"]["gteps_learned"], "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "grid4096_bfs_cc_selector", "nodes": g.nodes, "edges": g.edges,
+                       "remove": 0.05, "long_range": 0.001, "source": 0},
+            "results": out}
+    print(json.dumps(line), flush=True)
+    dg.free()
+
+
+def run_rmat26(args, rank: int, world: int, local: int):
+    """Config: RMAT scale 26, 64 seeded sources (degree >= 1) for BFS and SSSP,
+    CC once; learned selector vs the edge-balanced fixed style. Sources shard
+    across ranks."""
+    import torch
+
+    import indigo2suite_b200 as i2
+    from indigo2suite_b200 import shard
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    t0 = time.time()
+    dg = i2.DeviceGraph.generate_rmat(26, 16, 0.57, 0.19, 0.19, seed=26)
+    gen_s = time.time() - t0
+    if SELECTOR_PARAMS.exists():
+        i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
+    rng = np.random.default_rng(26)
+    srcs = []
+    while len(srcs) < 64:
+        v = int(rng.integers(0, dg.nodes))
+        if dg.degree(v) > 0:
+            srcs.append(v)
+    lo, hi = shard.shard_range(64, rank, world)
+    mine = srcs[lo:hi]
+    res = {}
+    for an, algo in (("bfs", i2.I2_BFS), ("sssp", i2.I2_SSSP), ("cc", i2.I2_CC)):
+        for v in ("vp_cta", "heuristic", "learned"):
+            ss = mine if algo != i2.I2_CC else mine[:1]
+            dg.run_device(algo, ss[0], variant=v, stream=sp, report=False)
+            torch.cuda.synchronize()
+            it = iter(ss)
+            t = _event_time(torch, stream, lambda: dg.run_device(algo, next(it), variant=v, stream=sp, report=False),
+                            len(ss))
+            t = dist.max(t, dev)
+            res[f"{an}/{v}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t}
+    line = {"metric": METRIC, "value": world * res["bfs/learned"]["gteps"], "unit": UNIT, "n_gpus": world,
+            "steps": 64, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "rmat26_bfs_sssp_cc_64src", "nodes": dg.nodes, "edges": dg.edges,
+                       "generation_s": gen_s, "parallelism": f"sources sharded x{world}"},
+            "results": res}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dg.free()
+    dist.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,6 +543,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-styles", action="store_true", help="skip the per-style comparison")
+    ap.add_argument("--workload", choices=["sssp_rmat22", "batch512", "grid4096", "rmat26"], default="sssp_rmat22",
+                    help="sssp_rmat22 is the benchmark line; the others are the other configurations")
     ap.add_argument("--loop", choices=["graph", "host"], default="graph",
                     help="device loop in one CUDA graph (default) or one host launch per iteration "
                          "(for per-kernel profiling)")
@@ -371,7 +556,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    run_ours(args, rank, world, local)
+    {"sssp_rmat22": run_ours, "batch512": run_batch512, "grid4096": run_grid4096,
+     "rmat26": run_rmat26}[args.workload](args, rank, world, local)
 
 
 if __name__ == "__main__":

@@ -157,6 +157,7 @@ int i2_graph_wrap_device(const i2_eclgraph* dev, i2_graph** out);
 int i2_graph_generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
                            int weighted, i2_graph** out);
 int i2_graph_size(const i2_graph* g, int* nodes, int* edges);
+int i2_graph_degree(const i2_graph* g, int v, int* deg);
 /* Statistics of the graph; the first call also checks symmetry (one pass over the CSR). */
 int i2_graph_info_get(const i2_graph* g, i2_graph_info* out);
 /* Copy the device CSR back to a host graph allocated by the callee. */
@@ -229,6 +230,10 @@ int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out);
 /* dist: host array of sum(nodes) ints, graph k's vertices at offset voff[k]. */
 int i2_batch_run(i2_batch* b, int algo, const int* srcs, int* dist, const i2_opts* opts, i2_report* rep);
 int i2_batch_offsets(const i2_batch* b, long long* voff);
+/* Same traversal with the result left on the device (asynchronous on
+   opts->stream when rep is NULL); i2_batch_result copies it to the host. */
+int i2_batch_run_device(i2_batch* b, int algo, const int* srcs, const i2_opts* opts, i2_report* rep);
+int i2_batch_result(i2_batch* b, int* dist, const i2_opts* opts);
 int i2_batch_free(i2_batch* b);
 
 #ifdef __cplusplus

@@ -195,6 +195,11 @@ class DeviceGraph:
         _check(lib.i2_graph_size(self._h, C.byref(n), C.byref(e)), "graph size")
         self.nodes, self.edges = n.value, e.value
 
+    def degree(self, v: int) -> int:
+        d = C.c_int()
+        _check(lib.i2_graph_degree(self._h, v, C.byref(d)), "degree")
+        return d.value
+
     @property
     def info(self) -> dict:
         """Graph statistics (the first query also checks symmetry on the device)."""
@@ -334,6 +339,24 @@ class Batch:
         if st != capi.I2_OK:
             raise I2Error(st, "batch run")
         return [dist[self.voff[k]:self.voff[k + 1]] for k in range(len(self.graphs))], _report(r, st)
+
+    def run_device(self, algo: int, srcs=None, variant="vp_cta", loop=I2_LOOP_GRAPH, stream=None,
+                   report: bool = True):
+        """Traversal of every graph with results left on the device."""
+        o = _opts(variant, loop, 0, 0, stream)
+        r = capi.Report()
+        self._srcs = np.ascontiguousarray(srcs, dtype=np.int32) if algo != I2_CC else None
+        st = lib.i2_batch_run_device(self._h, algo, _iptr(self._srcs) if self._srcs is not None else None,
+                                     C.byref(o), C.byref(r) if report else None)
+        if st != capi.I2_OK:
+            raise I2Error(st, "batch run")
+        return _report(r, st) if report else None
+
+    def result(self, stream=None):
+        dist = np.empty(self.nodes, np.int32)
+        o = _opts("vp_cta", I2_LOOP_GRAPH, 0, 0, stream)
+        _check(lib.i2_batch_result(self._h, _iptr(dist), C.byref(o)), "batch result")
+        return [dist[self.voff[k]:self.voff[k + 1]] for k in range(len(self.graphs))]
 
     def free(self):
         if self._h:

@@ -88,6 +88,7 @@ SIGNATURES = {
     "i2_graph_generate_rmat": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I,
                                     C.POINTER(_P)]),
     "i2_graph_size": (_I, [_P, _PI, _PI]),
+    "i2_graph_degree": (_I, [_P, _I, _PI]),
     "i2_graph_info_get": (_I, [_P, C.POINTER(GraphInfo)]),
     "i2_graph_download": (_I, [_P, _PG]),
     "i2_graph_synth_weights": (_I, [_P]),
@@ -109,6 +110,8 @@ SIGNATURES = {
     "i2_batch_upload": (_I, [_PG, _I, C.POINTER(_P)]),
     "i2_batch_run": (_I, [_P, _I, _PI, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_batch_offsets": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "i2_batch_run_device": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
+    "i2_batch_result": (_I, [_P, _PI, C.POINTER(Opts)]),
     "i2_batch_free": (_I, [_P]),
 }
 

@@ -127,6 +127,30 @@ int i2_batch_run(i2_batch* b, int algo, const int* srcs, int* dist, const i2_opt
   return st2 ? st2 : st;
 }
 
+int i2_batch_run_device(i2_batch* b, int algo, const int* srcs, const i2_opts* opts, i2_report* rep) {
+  if (!b) return I2_ERR_ARG;
+  if (algo != I2_CC && !srcs) return I2_ERR_ARG;
+  i2_graph_info info;
+  int n = 0, e = 0;
+  i2_graph_size(b->g, &n, &e);
+  (void)info;
+  std::vector<int> global;
+  if (algo != I2_CC) {
+    global.resize(b->n);
+    for (int k = 0; k < b->n; ++k) {
+      const long long nk = (k + 1 < b->n ? b->voff[k + 1] : n) - b->voff[k];
+      if (srcs[k] < 0 || srcs[k] >= nk) return I2_ERR_ARG;
+      global[k] = (int)(b->voff[k] + srcs[k]);
+    }
+  }
+  return run_traversal(b->g, algo, 0, algo == I2_CC ? nullptr : global.data(), b->n, opts, rep);
+}
+
+int i2_batch_result(i2_batch* b, int* dist, const i2_opts* opts) {
+  if (!b || !dist) return I2_ERR_ARG;
+  return graph_copy_result(b->g, dist, opts);
+}
+
 int i2_batch_free(i2_batch* b) {
   if (!b) return I2_ERR_ARG;
   i2_graph_free(b->g);

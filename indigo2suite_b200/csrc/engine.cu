@@ -317,7 +317,11 @@ __global__ void k_symmetry(DGraph g, const int* __restrict__ sp, DevStats* st) {
     const int v = g.nlist[k];
     int lo = g.nindex[v], hi = g.nindex[v + 1] - 1, pos = -1;
     while (lo <= hi) {
-      const int mid = (lo + hi) >> 1;
+      const int mid = lo + ((hi - lo) >> 1);  // lo + hi may exceed INT_MAX
+      if ((unsigned)mid >= (unsigned)g.edges) {
+        asym = 1;  // cannot happen on a validated CSR; refuse rather than read out of bounds
+        break;
+      }
       const int x = g.nlist[mid];
       if (x == u) { pos = mid; break; }
       if (x < u) lo = mid + 1; else hi = mid - 1;
@@ -333,7 +337,7 @@ __global__ void k_build_sp(DGraph g, int* sp) {
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
   for (long long v = warp; v < g.nodes; v += nwarps)
-    for (int k = g.nindex[v] + lane; k < g.nindex[v + 1]; k += 32) sp[k] = (int)v;
+    for (long long k = g.nindex[v] + lane; k < g.nindex[v + 1]; k += 32) sp[k] = (int)v;
 }
 
 // Reference synthetic weights (include/sssp_vertex_cuda.h:127-137) on the device.
@@ -1217,6 +1221,14 @@ int i2_graph_size(const i2_graph* g, int* nodes, int* edges) {
   if (!g || !nodes || !edges) return I2_ERR_ARG;
   *nodes = g->g.nodes;
   *edges = g->g.edges;
+  return I2_OK;
+}
+
+int i2_graph_degree(const i2_graph* g, int v, int* deg) {
+  if (!g || !deg || v < 0 || v >= g->g.nodes) return I2_ERR_ARG;
+  int pair[2];
+  I2_CK(cudaMemcpy(pair, g->g.nindex + v, sizeof(pair), cudaMemcpyDeviceToHost));
+  *deg = pair[1] - pair[0];
   return I2_OK;
 }
 

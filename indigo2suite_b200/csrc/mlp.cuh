@@ -23,7 +23,11 @@ constexpr int kOffW3 = kOffB2 + kHidden;
 constexpr int kOffB3 = kOffW3 + kHidden * kOut;
 constexpr int kParams = kOffB3 + kOut;
 
-// Features of a frontier about to be consumed. All are finite and O(1..40).
+// Features of a frontier about to be consumed. All are finite and O(1..30).
+// The graph-size features and the iteration index are clamped to the range the
+// selector is trained on (graphs of 2^16..2^20 vertices, frontiers reaching
+// their steady state within 64 iterations), so that bigger graphs and long
+// tails are treated like the largest trained ones instead of extrapolated.
 __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, int iter, int size, int hsize,
                                                   unsigned long long edges, int maxdeg, long long visited,
                                                   float* f) {
@@ -38,9 +42,9 @@ __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, in
   f[4] = log2f(1.f + fe / fmaxf(1.f, fs));
   f[5] = log2f(1.f + (float)maxdeg);
   f[6] = (float)visited / V;
-  f[7] = log2f(1.f + (float)iter);
-  f[8] = log2f(V);
-  f[9] = log2f(1.f + (float)gs.edges);
+  f[7] = log2f(1.f + fminf((float)iter, 64.f));
+  f[8] = fminf(fmaxf(log2f(V), 16.f), 20.f);
+  f[9] = fminf(fmaxf(log2f(1.f + (float)gs.edges), 17.f), 25.f);
   f[10] = log2f(1.f + gs.avgdeg);
   f[11] = log2f(1.f + (float)gs.maxdeg);
   f[12] = log2f(1.f + gs.degcv);

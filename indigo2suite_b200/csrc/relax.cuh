@@ -272,10 +272,11 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
   const int* __restrict__ ew = c.g.eweight;
   const int dus[4] = {du, du, du, du};
   if (c.g.vec_ok && hi - lo >= 8) {
-    const int q0 = lo >> 2;
-    const int q1 = (hi + 3) >> 2;
-    for (int q = q0 + lane; q < q1; q += gsize) {
-      const int k0 = q << 2;
+    // 64-bit index arithmetic: edges may come within a few units of INT_MAX
+    const long long q0 = lo >> 2;
+    const long long q1 = ((long long)hi + 3) >> 2;
+    for (long long q = q0 + lane; q < q1; q += gsize) {
+      const long long k0 = q << 2;
       int nv[4], wv[4] = {0, 0, 0, 0};
       bool ok[4];
       if (k0 + 3 < c.g.edges) {
@@ -290,7 +291,7 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
       } else {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          const int k = k0 + r;
+          const long long k = k0 + r;
           ok[r] = k >= lo && k < hi;
           nv[r] = ok[r] ? nl[k] : 0;
           if (Op<ALG>::kWeighted) wv[r] = ok[r] ? ew[k] : 0;
@@ -299,12 +300,12 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
       relax_batch<ALG, 4>(c, s, a, nxt, dus, nv, wv, ok);
     }
   } else {
-    for (int k0 = lo + lane * 4; k0 < hi; k0 += gsize * 4) {
+    for (long long k0 = lo + (long long)lane * 4; k0 < hi; k0 += (long long)gsize * 4) {
       int nv[4], wv[4] = {0, 0, 0, 0};
       bool ok[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        const int k = k0 + r;
+        const long long k = k0 + r;
         ok[r] = k < hi;
         nv[r] = ok[r] ? __ldg(nl + k) : 0;
         if (Op<ALG>::kWeighted) wv[r] = ok[r] ? __ldg(ew + k) : 0;
@@ -318,7 +319,7 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
 __device__ __forceinline__ int owner_search(const unsigned* __restrict__ off, int n, unsigned x) {
   int lo = 0, hi = n;
   while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
+    const int mid = lo + ((hi - lo) >> 1);
     if (off[mid] <= x) lo = mid; else hi = mid;
   }
   return lo;

@@ -245,6 +245,19 @@ def ref_cpu_run(name: str, g, src: int, threads: int, sp: np.ndarray | None = No
     if sp is None and "edge" in name:
         sp = globals()["sp"](g)
     out = np.empty(g.nodes, np.int32)
-    t = _cpu[name].ref_cpu_run(g.nodes, g.edges, _p(ni), _p(nl), _p(w) if w is not None else None, src, _p(out),
-                               _p(sp) if sp is not None else None, threads)
+    # the reference program prints progress on stdout; keep the caller's stdout clean
+    import sys
+
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        t = _cpu[name].ref_cpu_run(g.nodes, g.edges, _p(ni), _p(nl), _p(w) if w is not None else None, src,
+                                   _p(out), _p(sp) if sp is not None else None, threads)
+        C.CDLL(None).fflush(None)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
     return float(t), out
