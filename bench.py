@@ -44,6 +44,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "GTEPS & HBM GB/s: learned-style vs best fixed style, BFS/SSSP/CC bit-exact"
 UNIT = "GTEPS"
+# kernel that runs each style's iterations
+KERNEL_NAMES = {"vp_thread": "relax_push", "vp_warp": "relax_push", "vp_cta": "relax_edge_balanced",
+                "vp_block": "relax_push", "pull_frontier": "relax_pull", "pull_topo": "relax_pull",
+                "edge_topo": "relax_edge_topo", "push_topo": "relax_push_topo"}
 WORKLOAD = {"workload": "sssp_rmat22_ef16_edge_data_push", "graph": "rmat", "scale": 22, "edge_factor": 16,
             "a": 0.57, "b": 0.19, "c": 0.19, "seed": 22, "weights": "uniform[1,255]",
             "source": "highest-degree vertex", "algorithm": "sssp", "style": "vp_cta (edge-centric data-driven push)",
@@ -224,18 +228,20 @@ def run_ours(args, rank: int, world: int, local: int):
     variant = args.variant
 
     # correctness of the measured configuration (shortest-path certificate)
-    d, rep = dg.sssp(src, variant=variant)
+    delta = args.delta
+    d, rep = dg.sssp(src, variant=variant, delta=delta)
     import oracle
 
     cert = oracle.certify_distances(host, src, d, weighted=True)
     if cert is not None:
         raise SystemExit(f"result certificate failed: {cert}")
 
-    loop = i2.I2_LOOP_HOST if args.loop == "host" else i2.I2_LOOP_GRAPH
+    loop = {"graph": i2.I2_LOOP_GRAPH, "host": i2.I2_LOOP_HOST, "relaunch": i2.I2_LOOP_RELAUNCH}[args.loop]
 
     def steps(n, v=variant):
         for _ in range(n):
-            dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, loop=loop, report=loop == i2.I2_LOOP_HOST)
+            dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, loop=loop, report=loop == i2.I2_LOOP_HOST,
+                          delta=delta)
 
     with torch.cuda.stream(stream):
         steps(args.warmup)
@@ -257,22 +263,34 @@ def run_ours(args, rank: int, world: int, local: int):
     ms_max = dist.max(ms, dev)
     value = world * 1e-9 * E / (ms_max * 1e-3)
 
-    # dominant kernel: relax launches timed one by one with CUDA events (host-driven loop)
-    rep_h = dg.run_device(i2.I2_SSSP, src, variant=variant, loop=i2.I2_LOOP_HOST, stream=sp)
-    rep_g = dg.run_device(i2.I2_SSSP, src, variant=variant, stream=sp)
+    # Dominant kernel. With the graph loop one resident launch runs every
+    # iteration of a step, so its duration is the step's (CUDA events on the
+    # launching stream, over the timed region; the reset/fill/seed launches
+    # before it are < 2% of the step and are charged to it). The host-driven
+    # loop's per-iteration launches, each bracketed by CUDA events, are
+    # reported beside it.
+    rep_h = dg.run_device(i2.I2_SSSP, src, variant=variant, loop=i2.I2_LOOP_HOST, stream=sp, delta=delta)
+    rep_g = dg.run_device(i2.I2_SSSP, src, variant=variant, stream=sp, delta=delta)
     b_alg = 12.0 * rep_g.reached_edges + 20.0 * rep_g.reached_vertices
-    achieved = b_alg / rep_h.relax_seconds / 1e9
+    graph_loop = loop == i2.I2_LOOP_GRAPH
+    kernel_s = ms_max * 1e-3 if graph_loop else rep_h.relax_seconds
+    achieved = b_alg / kernel_s / 1e9
     peak, peak_kind = peaks()
+    kname = KERNEL_NAMES.get(variant, str(variant))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "peak_source": peak_kind,
-                "kernel": f"relax_push<SSSP,{variant}>", "launches_per_step": rep_g.iterations,
-                "b_alg_bytes_per_step": b_alg, "relax_ms_per_step_events": 1e3 * rep_h.relax_seconds,
-                "relax_ms_per_step_device_timer": 1e3 * rep_g.relax_seconds}
+                "kernel": (f"relax_resident<SSSP,{variant}>" if graph_loop else kname + "<SSSP>"),
+                "launches_per_step": 1 if graph_loop else rep_h.iterations, "iterations": rep_g.iterations,
+                "b_alg_bytes_per_step": b_alg, "kernel_ms_per_step": 1e3 * kernel_s,
+                "host_loop": {"kernel": kname + "<SSSP>", "launches": rep_h.iterations,
+                              "relax_ms_events": 1e3 * rep_h.relax_seconds,
+                              "achieved_gbs": b_alg / rep_h.relax_seconds / 1e9}}
     prof = ROOT / "profiles" / "relax_sssp_rmat22_traffic.json"
     if prof.exists():
         tr = json.loads(prof.read_text())
-        roofline["traffic"] = tr.get("dram_bytes_per_step")
-        roofline["traffic_note"] = tr.get("note")
+        if tr.get("kernel") == roofline["kernel"]:  # a capture of this configuration's kernel
+            roofline["traffic"] = tr.get("dram_bytes_per_launch")
+            roofline["traffic_note"] = tr.get("note")
 
     # the other styles and the selectors (a few steps each)
     styles = {}
@@ -303,7 +321,7 @@ def run_ours(args, rank: int, world: int, local: int):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         gg = i2.DeviceGraph.upload(hp)
-        gg.sssp(src, variant=variant, out=out)
+        gg.sssp(src, variant=variant, out=out, delta=delta)
         gg.free()
         torch.cuda.synchronize()
         if k > 0:
@@ -315,7 +333,7 @@ def run_ours(args, rank: int, world: int, local: int):
            "query_only_note": "per-query C-ABI call on a resident graph: see e2e_query"}
     q0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        dg.sssp(src, variant=variant, out=out)
+        dg.sssp(src, variant=variant, out=out, delta=delta)
     q_s = (time.perf_counter() - q0) / args.e2e_steps
     e2e_query = {"value": world * 1e-9 * E / dist.max(q_s, dev), "unit": UNIT, "h2d_bytes_per_step": 4,
                  "d2h_bytes_per_step": 4 * V}
@@ -332,12 +350,13 @@ def run_ours(args, rank: int, world: int, local: int):
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
 
-    launches = args.steps * (3 + rep_g.iterations)
+    # per step: k_reset, k_fill, k_seed and the relax launch(es)
+    launches = args.steps * (3 + (1 if graph_loop else rep_g.iterations))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}",
-                           loop=args.loop),
+                           loop=args.loop, near_far_step=delta if delta > 0 else "off"),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_query": e2e_query,
             "gpu_launches": launches, "clocks": clk,
             "styles_gteps": styles, "best_fixed_style": max(fixed, key=fixed.get),
@@ -539,15 +558,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--variant", default="vp_cta")
+    ap.add_argument("--delta", type=int, default=0,
+                    help="SSSP near/far threshold step of the vp_cta style: <= 0 off, > 0 this step")
     ap.add_argument("--style-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-styles", action="store_true", help="skip the per-style comparison")
     ap.add_argument("--workload", choices=["sssp_rmat22", "batch512", "grid4096", "rmat26"], default="sssp_rmat22",
                     help="sssp_rmat22 is the benchmark line; the others are the other configurations")
-    ap.add_argument("--loop", choices=["graph", "host"], default="graph",
-                    help="device loop in one CUDA graph (default) or one host launch per iteration "
-                         "(for per-kernel profiling)")
+    ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
+                    help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
+                         "host: one host launch per iteration; relaunch: one launch per iteration "
+                         "from the graph's device-side loop")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if world != args.gpus and not (world == 1 and args.gpus == 1):

@@ -37,7 +37,9 @@ typedef enum {
   I2_ERR_UNSUPPORTED = 7, /* variant not applicable to this graph (pull on a directed graph) */
   I2_ERR_ITER_CAP = 8,    /* iteration cap reached before the fixed point */
   I2_ERR_OVERFLOW = 9,    /* int32 limit or capacity exceeded */
-  I2_ERR_CAPACITY = 10    /* graph larger than i2_run_noalloc's fixed scratch */
+  I2_ERR_CAPACITY = 10,   /* graph larger than i2_run_noalloc's fixed scratch */
+  I2_ERR_STALL = 11       /* a resident traversal's barrier wait ran out of time
+                             (I2_STALL_MS, default 10 s); the result is incomplete */
 } i2_status;
 
 /* Host CSR graph. Layout-identical to struct ECLgraph (include/ECLgraph.h:44-50). */
@@ -69,8 +71,12 @@ enum {
 
 /* Loop modes. */
 enum {
-  I2_LOOP_GRAPH = 0, /* whole traversal is one CUDA graph with a device-side while loop */
-  I2_LOOP_HOST = 1   /* host launches each iteration and reads the frontier size back */
+  I2_LOOP_GRAPH = 0,   /* whole traversal is one CUDA graph; its relax kernel is one
+                          cooperative launch that runs every iteration, the grid
+                          meeting at a barrier between iterations */
+  I2_LOOP_HOST = 1,    /* host launches each iteration and reads the frontier size back */
+  I2_LOOP_RELAUNCH = 2 /* one CUDA graph with a device-side while loop that launches
+                          the relax kernel once per iteration */
 };
 
 typedef struct {
@@ -79,6 +85,11 @@ typedef struct {
   int iter_cap;     /* 0: default cap of nodes + 2 launches (enough for every algorithm) */
   int record_iters; /* 1: keep per-iteration records (i2_get_records) */
   void* stream;     /* cudaStream_t to run on; NULL: the graph's own stream */
+  int sssp_delta;   /* SSSP with I2_VP_CTA only: threshold step of the near/far
+                       ordering (pushes at or above the threshold wait on a far
+                       pile until the near frontier is empty). <= 0: off
+                       (plain frontier-driven relaxation), > 0: this step.
+                       The distances do not depend on it. */
 } i2_opts;
 
 typedef struct {

@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi as capi
-from ._capi import (I2_AUTO_HEURISTIC, I2_AUTO_LEARNED, I2_BFS, I2_CC, I2_LOOP_GRAPH, I2_LOOP_HOST,
+from ._capi import (I2_AUTO_HEURISTIC, I2_AUTO_LEARNED, I2_BFS, I2_CC, I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH,
                     I2_NUM_VARIANTS, I2_SSSP, VARIANTS)
 
 lib = capi.load()
@@ -34,7 +34,7 @@ __all__ = [
     "gen_grid", "gen_rmat_n", "synth_weights", "build_sp", "VARIANTS", "variant_id", "GPUbfs_vertex", "GPUbfs_edge",
     "GPUsssp_vertex", "GPUsssp_edge", "GPUcc_vertex", "GPUcc_edge", "mlp_param_count", "mlp_loss_grad",
     "mlp_train", "mlp_predict", "mlp_set_params", "device_count", "I2_BFS", "I2_SSSP", "I2_CC",
-    "I2_AUTO_HEURISTIC", "I2_AUTO_LEARNED", "I2_NUM_VARIANTS", "I2_LOOP_GRAPH", "I2_LOOP_HOST",
+    "I2_AUTO_HEURISTIC", "I2_AUTO_LEARNED", "I2_NUM_VARIANTS", "I2_LOOP_GRAPH", "I2_LOOP_HOST", "I2_LOOP_RELAUNCH",
 ]
 
 INF = np.iinfo(np.int32).max
@@ -175,9 +175,10 @@ class Report:
     status: int = 0
 
 
-def _opts(variant, loop, iter_cap, record, stream) -> capi.Opts:
+def _opts(variant, loop, iter_cap, record, stream, delta: int = 0) -> capi.Opts:
+    """delta: SSSP near/far threshold step for the vp_cta style (<= 0 off, > 0 this step)."""
     return capi.Opts(variant_id(variant), int(loop), int(iter_cap), int(record),
-                     C.c_void_p(stream) if stream else None)
+                     C.c_void_p(stream) if stream else None, int(delta))
 
 
 def _report(r: capi.Report, status: int) -> Report:
@@ -256,10 +257,10 @@ class DeviceGraph:
             pass
 
     # -- traversals ---------------------------------------------------------
-    def _run(self, algo: int, src: int, variant, loop, iter_cap, record, stream, out=None):
+    def _run(self, algo: int, src: int, variant, loop, iter_cap, record, stream, out=None, delta=0):
         dist = out if out is not None else np.empty(self.nodes, np.int32)
         assert dist.dtype == np.int32 and dist.size >= self.nodes and dist.flags.c_contiguous
-        o = _opts(variant, loop, iter_cap, record, stream)
+        o = _opts(variant, loop, iter_cap, record, stream, delta)
         r = capi.Report()
         if algo == I2_BFS:
             st = lib.i2_bfs(self._h, src, _iptr(dist), C.byref(o), C.byref(r))
@@ -274,17 +275,18 @@ class DeviceGraph:
     def bfs(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
         return self._run(I2_BFS, src, variant, loop, iter_cap, record, stream, out)
 
-    def sssp(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
-        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out)
+    def sssp(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
+             delta: int = 0):
+        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out, delta)
 
     def cc(self, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
         return self._run(I2_CC, 0, variant, loop, iter_cap, record, stream, out)
 
     def run_device(self, algo: int, src: int = 0, out_ptr: int = 0, variant="vp_cta", loop=I2_LOOP_GRAPH,
-                   iter_cap=0, record=False, stream=None, report: bool = True) -> Report | None:
+                   iter_cap=0, record=False, stream=None, report: bool = True, delta: int = 0) -> Report | None:
         """Traversal with the result left in device memory (copied to out_ptr if given).
         With report=False and the graph loop the call is asynchronous on `stream`."""
-        o = _opts(variant, loop, iter_cap, record, stream)
+        o = _opts(variant, loop, iter_cap, record, stream, delta)
         r = capi.Report()
         st = lib.i2_run_device(self._h, algo, src, C.c_void_p(out_ptr) if out_ptr else None, C.byref(o),
                                C.byref(r) if report else None)

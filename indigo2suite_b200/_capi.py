@@ -7,9 +7,11 @@ or cannot be loaded, importing this module raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libi2b200.so"
+# I2B200_LIB selects another build of the library (e.g. one with other tuning constants)
+LIB_PATH = Path(os.environ.get("I2B200_LIB") or Path(__file__).resolve().parent / "libi2b200.so")
 
 I2_OK = 0
 I2_ERR_ARG = 1
@@ -22,6 +24,7 @@ I2_ERR_UNSUPPORTED = 7
 I2_ERR_ITER_CAP = 8
 I2_ERR_OVERFLOW = 9
 I2_ERR_CAPACITY = 10
+I2_ERR_STALL = 11
 
 I2_BFS, I2_SSSP, I2_CC = 0, 1, 2
 
@@ -29,7 +32,7 @@ I2_AUTO_HEURISTIC = -1
 I2_AUTO_LEARNED = -2
 VARIANTS = ["vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo", "edge_topo", "push_topo"]
 I2_NUM_VARIANTS = len(VARIANTS)
-I2_LOOP_GRAPH, I2_LOOP_HOST = 0, 1
+I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH = 0, 1, 2
 
 NUM_FEATURES = 16
 
@@ -41,7 +44,7 @@ class EclGraphC(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("variant", C.c_int), ("loop_mode", C.c_int), ("iter_cap", C.c_int),
-                ("record_iters", C.c_int), ("stream", C.c_void_p)]
+                ("record_iters", C.c_int), ("stream", C.c_void_p), ("sssp_delta", C.c_int)]
 
 
 class Report(C.Structure):

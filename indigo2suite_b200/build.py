@@ -48,23 +48,32 @@ def _headers() -> list[Path]:
     return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
 
 
-def _stale(obj: Path, src: Path) -> bool:
+def _stale(obj: Path, src: Path, flags_file: Path) -> bool:
     if not obj.exists():
         return True
     t = obj.stat().st_mtime
-    return any(p.stat().st_mtime > t for p in [src, *_headers(), Path(__file__)])
+    return any(p.stat().st_mtime > t for p in [src, *_headers(), Path(__file__), flags_file])
 
 
-def build(verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, defines=(), out: Path | None = None, build_dir: Path | None = None) -> Path:
+    """Compile the library. `defines` (NAME=VALUE strings) override the
+    engine's compile-time tuning constants (for example I2_EB_MIN_BLOCKS);
+    such builds should go to their own `out` and `build_dir`."""
+    lib = Path(out) if out else LIB
+    bdir = Path(build_dir) if build_dir else BUILD
+    bdir.mkdir(parents=True, exist_ok=True)
+    dflags = [f"-D{d}" for d in defines]
+    flags_file = bdir / "defines.txt"
+    if not flags_file.exists() or flags_file.read_text() != " ".join(dflags):
+        flags_file.write_text(" ".join(dflags))
     objs = []
     procs = []
     for name in SOURCES:
         src = CSRC / name
-        obj = BUILD / (name + ".o")
+        obj = bdir / (name + ".o")
         objs.append(obj)
-        if _stale(obj, src):
-            cmd = [nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        if _stale(obj, src, flags_file):
+            cmd = [nvcc(), *NVCC_FLAGS, *dflags, "-c", str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             procs.append((name, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
@@ -78,15 +87,22 @@ def build(verbose: bool = False) -> Path:
     if failed:
         msg = "\n".join(f"--- {n}\n{o}" for n, o in failed)
         raise RuntimeError("nvcc failed:\n" + msg)
-    if procs or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC,-fopenmp", "-o", str(LIB),
+    if procs or not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC,-fopenmp", "-o", str(lib),
                *[str(o) for o in objs], "-lgomp"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv)
-    print(LIB)
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-v", action="store_true")
+    ap.add_argument("-D", action="append", default=[], metavar="NAME=VALUE")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--build-dir", default=None)
+    a = ap.parse_args()
+    print(build(verbose=a.v, defines=a.D, out=a.out, build_dir=a.build_dir))

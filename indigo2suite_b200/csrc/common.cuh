@@ -21,6 +21,11 @@
 //   the current dist[]. Iteration i propagates at least F_i and builds F_{i+1}
 //   in slot (i+1) % 3 from every vertex whose value it lowered. It also clears
 //   slot (i+2) % 3 (F_{i-1}), which no variant reads during iteration i.
+// SSSP near/far ordering (Ctl::delta > 0) relaxes the contract in one way: a
+// lowered vertex whose new distance is at or above the current threshold goes
+// onto the far pile instead of F_{i+1}. The traversal ends when both F_{i+1}
+// and the pile are empty. Only the edge-balanced push defers; every other
+// variant pushes all lowered vertices into F_{i+1}, which is always valid.
 #pragma once
 #include <cstdint>
 #include <climits>
@@ -73,6 +78,7 @@ struct GStats {
   int symmetric;    // 1 when every (u,v,w) has a (v,u,w) partner
   float avgdeg;
   float degcv;      // coefficient of variation of the degree distribution
+  float wmean;      // mean edge weight (1 for BFS)
 };
 
 // Statistics of one frontier buffer, accumulated while it is built. Entries
@@ -112,6 +118,26 @@ struct Ctl {
   int sel_n;                // frontier entries at the last selector evaluation
   unsigned sel_e;           // frontier edges at the last selector evaluation
   int sel_iter;             // iteration of the last selector evaluation
+  // SSSP near/far ordering (delta > 0 only): relax iterations push values at
+  // or above `threshold` onto far pile `pcur` instead of the next frontier;
+  // when the next frontier is empty and the pile is not, the next launch is a
+  // split (split = 1): the threshold rises to max(threshold, pmin) + delta and
+  // the pile's entries below it move into the next frontier, the others onto
+  // the other pile.
+  int delta;
+  int threshold;
+  int prev_threshold;       // threshold before the last rise
+  int split;
+  int pcur;
+  unsigned psize[2];
+  int pmin[2];              // lower bound of the values on each pile
+  // Resident launches (one launch runs every iteration, the grid meeting at
+  // a barrier between them).
+  unsigned bar_gen;         // barrier generation, bumped once per iteration
+  int go;                   // 1 while another iteration follows
+  int hold;                 // test hook: the first release is withheld
+  int pad1;
+  unsigned long long stall_ns;  // longest wait at the barrier before giving up
   unsigned long long relax_ns;  // sum of relax launch durations
   float feat[kFeatures];    // features of the frontier the next launch consumes
 };
@@ -119,6 +145,7 @@ struct Ctl {
 enum : int {
   kStatusIterCap = 1,
   kStatusOverflow = 2,
+  kStatusStall = 4,  // a resident launch's barrier wait ran out of time
 };
 
 // One record per relax launch: the frontier it consumed and its duration.
@@ -144,6 +171,8 @@ struct Ctx {
   unsigned* woff[3];
   int* hwl[3];
   unsigned* htoff[3];
+  int* pile[2];             // far piles (SSSP near/far ordering), vertices
+  unsigned* fbm;            // bit set: vertex is on the current far pile
   unsigned* bm[3];
   Ctl* ctl;
   IterRec* recs;

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -99,6 +100,7 @@ __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
     }
     ctl->variant = v;
     if (cond) ctl->hist[v] += 1;
+    ctl->go = cond ? 1 : 0;
     if (c.use_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)c.loop_h, cond ? 1u : 0u);
   }
 }
@@ -139,6 +141,24 @@ __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old)
     volatile Slot* sn = &ctl->slot[nxt];
     const long long n = slot_size(sn->packed);
     int cond = n > 0;
+    if (ctl->delta > 0) {
+      if (ctl->split) {  // this launch emptied pile pcur onto the other one
+        const int p = ctl->pcur;
+        ctl->psize[p] = 0;
+        ctl->pmin[p] = kInf;
+        ctl->pcur = 1 - p;
+        ctl->split = 0;
+      }
+      const int p = ctl->pcur;
+      if (n == 0 && *(volatile unsigned*)&ctl->psize[p] > 0) {
+        // next launch splits the pile at a raised threshold
+        const long long lo = max((long long)ctl->threshold, (long long)*(volatile int*)&ctl->pmin[p]);
+        ctl->prev_threshold = ctl->threshold;
+        ctl->threshold = (int)min(lo + (long long)ctl->delta, (long long)kInf);
+        ctl->split = 1;
+        cond = 1;
+      }
+    }
     if (cond && i + 1 >= ctl->iter_cap) {
       ctl->status |= kStatusIterCap;
       cond = 0;
@@ -230,7 +250,7 @@ __global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
 // Per-run parameters, passed by value to k_reset so that queued runs never
 // share a host buffer.
 struct RunParams {
-  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap;
+  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap, delta, hold, stall_ms;
   bool operator!=(const RunParams& o) const { return std::memcmp(this, &o, sizeof(RunParams)) != 0; }
 };
 
@@ -248,6 +268,12 @@ __global__ void k_reset(Ctl* ctl, RunParams p) {
   ctl->src = p.src;
   ctl->nsrc = p.nsrc;
   ctl->algo = p.algo;
+  ctl->delta = p.delta;
+  ctl->hold = p.hold;
+  ctl->stall_ns = (unsigned long long)p.stall_ms * 1000000ull;
+  ctl->threshold = p.delta > 0 ? p.delta : kInf;  // sources start at 0
+  ctl->pmin[0] = kInf;
+  ctl->pmin[1] = kInf;
 }
 
 // ---------------------------------------------------------------------------
@@ -271,6 +297,7 @@ struct DevStats {
   int asym;
   int pad;
   double sumsq;
+  double wsum;
 };
 
 __global__ void k_degree_stats(DGraph g, int heavy, DevStats* st) {
@@ -286,9 +313,15 @@ __global__ void k_degree_stats(DGraph g, int heavy, DevStats* st) {
     s2 += (double)d * d;
   }
   int wmin = INT_MAX;
+  double ws = 0.0;
   if (g.eweight)
-    for (long long e = tid; e < g.edges; e += stride) wmin = min(wmin, g.eweight[e]);
+    for (long long e = tid; e < g.edges; e += stride) {
+      const int w = g.eweight[e];
+      wmin = min(wmin, w);
+      ws += (double)w;
+    }
   atomicMax(&st->maxdeg, mx);
+  atomicAdd(&st->wsum, ws);
   atomicAdd(&st->nheavy, nh);
   atomicMin(&st->wmin, wmin);
   if (uns) atomicOr(&st->unsorted, 1);
@@ -398,7 +431,32 @@ static KernelFn dispatch_kernel(int algo) {
   return relax_dispatch<kCC>;
 }
 
-KernelFn relax_kernel(int algo, int v) {
+template <int ALG>
+static KernelFn resident_fn(int v) {
+  switch (v) {
+    case kVPThread: return relax_resident<ALG, kVPThread>;
+    case kVPWarp: return relax_resident<ALG, kVPWarp>;
+    case kVPCta: return relax_resident<ALG, kVPCta>;
+    case kVPBlock: return relax_resident<ALG, kVPBlock>;
+    case kPullFrontier: return relax_resident<ALG, kPullFrontier>;
+    case kPullTopo: return relax_resident<ALG, kPullTopo>;
+    case kEdgeTopo: return relax_resident<ALG, kEdgeTopo>;
+    case kPushTopo: return relax_resident<ALG, kPushTopo>;
+  }
+  return relax_resident<ALG, -1>;  // per-iteration pick
+}
+
+// Kernel of a resident traversal: fixed style v (mode 0) or the per-iteration
+// pick (v < 0).
+static KernelFn resident_kernel(int algo, int v, bool near_far) {
+  if (near_far && algo == kSSSP && v == kVPCta) return relax_resident<kSSSP, kVPCta, true>;
+  if (algo == kBFS) return resident_fn<kBFS>(v);
+  if (algo == kSSSP) return resident_fn<kSSSP>(v);
+  return resident_fn<kCC>(v);
+}
+
+KernelFn relax_kernel(int algo, int v, bool near_far) {
+  if (near_far && algo == kSSSP && v == kVPCta) return relax_near_far;
   if (algo == kBFS) return relax_fn<kBFS>(v);
   if (algo == kSSSP) return relax_fn<kSSSP>(v);
   return relax_fn<kCC>(v);
@@ -488,12 +546,14 @@ using namespace i2;
 // Graph handle.
 
 struct ExecKey {
-  int algo, mode, variant, multi;
+  int algo, mode, variant, multi, near_far, resident;
   bool operator<(const ExecKey& o) const {
     if (algo != o.algo) return algo < o.algo;
     if (mode != o.mode) return mode < o.mode;
     if (variant != o.variant) return variant < o.variant;
-    return multi < o.multi;
+    if (multi != o.multi) return multi < o.multi;
+    if (near_far != o.near_far) return near_far < o.near_far;
+    return resident < o.resident;
   }
 };
 
@@ -524,7 +584,10 @@ struct i2_graph {
   int* hwl[3] = {nullptr, nullptr, nullptr};
   unsigned* htoff[3] = {nullptr, nullptr, nullptr};
   unsigned* bm[3] = {nullptr, nullptr, nullptr};
+  unsigned* fbm = nullptr;  // far-pile bitmap, allocated after bm[2]
+  int* pile[2] = {nullptr, nullptr};
   int bm_words = 0;
+  bool resident_ok = true;  // cleared if the device refuses the cooperative loop node
   Ctl* ctl = nullptr;
   IterRec* recs = nullptr;
   int rec_cap = 0;
@@ -563,6 +626,8 @@ static void free_graph_state(i2_graph* g) {
     cudaFree(g->htoff[k]);
   }
   cudaFree(g->bm[0]);
+  cudaFree(g->pile[0]);
+  cudaFree(g->pile[1]);
   cudaFree(g->ctl);
   cudaFree(g->recs);
   cudaFree(g->srcs);
@@ -609,6 +674,7 @@ static int compute_stats(i2_graph* g) {
   const double var = std::max(0.0, h.sumsq / (double)g->g.nodes - mean * mean);
   s.avgdeg = (float)mean;
   s.degcv = mean > 0 ? (float)(std::sqrt(var) / mean) : 0.f;
+  s.wmean = (g->g.eweight && g->g.edges > 0) ? (float)(h.wsum / (double)g->g.edges) : 1.f;
   return I2_OK;
 }
 
@@ -636,13 +702,21 @@ static int ensure_workspace(i2_graph* g) {
     I2_CK(cudaMalloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
   }
   unsigned* bm = nullptr;
-  I2_CK(cudaMalloc(&bm, sizeof(unsigned) * 3ull * g->bm_words));
+  I2_CK(cudaMalloc(&bm, sizeof(unsigned) * 4ull * g->bm_words));
   for (int k = 0; k < 3; ++k) g->bm[k] = bm + (size_t)k * g->bm_words;
+  g->fbm = bm + 3ull * g->bm_words;
   I2_CK(cudaMalloc(&g->ctl, sizeof(Ctl)));
   g->rec_cap = (int)std::min<long long>(V + 2, 1 << 16);
   I2_CK(cudaMalloc(&g->recs, sizeof(IterRec) * g->rec_cap));
   I2_CK(cudaMalloc(&g->reach, sizeof(unsigned long long) * 2));
   g->ws_ready = true;
+  return I2_OK;
+}
+
+static int ensure_piles(i2_graph* g) {
+  if (g->pile[0]) return I2_OK;
+  for (int k = 0; k < 2; ++k) I2_CK(cudaMalloc(&g->pile[k], sizeof(int) * ((size_t)g->g.nodes + 1)));
+  drop_execs(g);  // graphs bake the context
   return I2_OK;
 }
 
@@ -707,20 +781,45 @@ static Ctx make_ctx(const i2_graph* g) {
   c.rec_cap = g->rec_cap;
   c.heavy = g->heavy;
   c.bm_words = g->bm_words;
+  c.pile[0] = g->pile[0];
+  c.pile[1] = g->pile[1];
+  c.fbm = g->fbm;
   c.mlp = mlp_device_params();
   c.srcs = nullptr;
   return c;
 }
 
-static RunParams make_params(const i2_graph* g, int algo, int mode, int variant, int src, int nsrc, int cap) {
-  RunParams p;
+// Near/far ordering applies to SSSP with the fixed edge-balanced push only
+// (the style that implements the split launches), and only when the caller
+// asks for it: it relaxes up to 2.2x fewer edges on RMAT graphs, but each
+// split rescans the far pile and every threshold step adds launches, which
+// measured slower than plain frontier-driven relaxation on RMAT, ER and grid
+// graphs of 2^18..2^22 vertices at every step tried.
+static int pick_delta(const i2_graph* g, int algo, int mode, int variant, int requested) {
+  (void)g;
+  if (algo != I2_SSSP || mode != 0 || variant != kVPCta || requested <= 0) return 0;
+  return requested;
+}
+
+static RunParams make_params(const i2_graph* g, int algo, int mode, int variant, int src, int nsrc, int cap,
+                             int delta = 0) {
+  RunParams p{};
   p.algo = algo;
   p.mode = mode;
   p.fixed_variant = variant < 0 ? 0 : variant;
   p.allowed = allowed_mask(g);
   p.src = src;
   p.nsrc = nsrc;
-  p.iter_cap = cap > 0 ? cap : g->g.nodes + 2;
+  p.delta = delta;
+  // Test hook: withhold the first barrier release of a resident traversal,
+  // so that every block's bounded wait runs out (I2_STALL_MS bounds it).
+  const char* hold = std::getenv("I2_TEST_HOLD_BARRIER");
+  p.hold = (hold && hold[0] == '1') ? 1 : 0;
+  const char* stall = std::getenv("I2_STALL_MS");
+  p.stall_ms = stall ? std::max(1, std::atoi(stall)) : 10000;
+  // a split launch moves at least one pile entry into a frontier, or learns
+  // the pile's exact minimum for the next one
+  p.iter_cap = cap > 0 ? cap : (int)std::min<long long>((long long)g->g.nodes * (delta > 0 ? 3 : 1) + 2, INT_MAX);
   return p;
 }
 
@@ -738,9 +837,9 @@ static int add_kernel_node(cudaGraph_t gr, cudaGraphNode_t* node, const cudaGrap
   return I2_OK;
 }
 
-static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, const RunParams& rp,
+static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, bool resident, const RunParams& rp,
                       ExecEntry** out) {
-  ExecKey key{algo, mode, mode == 0 ? variant : -1, multi ? 1 : 0};
+  ExecKey key{algo, mode, mode == 0 ? variant : -1, multi ? 1 : 0, rp.delta > 0 ? 1 : 0, resident ? 1 : 0};
   auto it = g->execs.find(key);
   if (it != g->execs.end()) {
     *out = &it->second;
@@ -761,7 +860,7 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   ms.dst = g->bm[0];
   ms.value = 0;
   ms.elementSize = 4;
-  ms.width = 3ull * g->bm_words;
+  ms.width = 4ull * g->bm_words;  // frontier and far-pile bitmaps
   ms.height = 1;
   ms.pitch = 0;
   I2_CK(cudaGraphAddMemsetNode(&n_ms, gr, nullptr, 0, &ms));
@@ -788,13 +887,22 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   cp.conditional.size = 1;
   I2_CK(cudaGraphAddNode(&n_loop, gr, &n_seed, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // The loop body is one kernel: the fixed style's, or the dispatch kernel
-  // whose blocks branch on the style the previous iteration selected.
+  // The loop body is one kernel. Resident: a cooperative launch that runs
+  // every iteration itself (the loop then runs once). Otherwise one launch per
+  // iteration: the fixed style's kernel, or the dispatch kernel whose blocks
+  // branch on the style the previous iteration selected.
   {
     cudaGraphNode_t n;
-    KernelFn fn = mode == 0 ? relax_kernel(algo, variant) : dispatch_kernel(algo);
+    KernelFn fn = resident ? resident_kernel(algo, mode == 0 ? variant : -1, rp.delta > 0)
+                  : mode == 0 ? relax_kernel(algo, variant, rp.delta > 0)
+                              : dispatch_kernel(algo);
     st = add_kernel_node(body, &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
     if (st) return st;
+    if (resident) {
+      cudaKernelNodeAttrValue av{};
+      av.cooperative = 1;
+      I2_CK(cudaGraphKernelNodeSetAttribute(n, cudaKernelNodeAttributeCooperative, &av));
+    }
   }
   ExecEntry e;
   I2_CK(cudaGraphInstantiate(&e.ex, gr, 0));
@@ -827,7 +935,7 @@ static int launch_exec(i2_graph* g, ExecEntry* e, const RunParams& rp, cudaStrea
 
 // Reset the bitmaps and the control block on the stream (host-driven paths).
 static int prepare_run(i2_graph* g, cudaStream_t s, const RunParams& rp) {
-  I2_CK(cudaMemsetAsync(g->bm[0], 0, sizeof(unsigned) * 3ull * g->bm_words, s));
+  I2_CK(cudaMemsetAsync(g->bm[0], 0, sizeof(unsigned) * 4ull * g->bm_words, s));
   k_reset<<<1, 32, 0, s>>>(g->ctl, rp);
   I2_CK(cudaGetLastError());
   return I2_OK;
@@ -849,8 +957,8 @@ static int run_host_loop(i2_graph* g, cudaStream_t s, int algo, bool multi, doub
     I2_CK(cudaStreamSynchronize(s));
     const int cur = h->iter % 3;
     const long long n = slot_size(h->slot[cur].packed);
-    if (n == 0 || (h->status & kStatusIterCap)) break;
-    KernelFn fn = relax_kernel(algo, h->variant);
+    if ((n == 0 && !h->split) || (h->status & kStatusIterCap)) break;
+    KernelFn fn = relax_kernel(algo, h->variant, h->delta > 0);
     I2_CK(cudaEventRecord(g->ev2, s));
     fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
     I2_CK(cudaGetLastError());
@@ -883,6 +991,7 @@ static int fill_report(i2_graph* g, cudaStream_t s, int algo, i2_report* rep, do
     rep->reached_vertices = (long long)r[0];
     rep->reached_edges = (long long)r[1];
   }
+  if (h->status & kStatusStall) return I2_ERR_STALL;
   if (h->status & kStatusIterCap) return I2_ERR_ITER_CAP;
   (void)algo;
   return I2_OK;
@@ -895,6 +1004,7 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   I2_CK(cudaSetDevice(g->device));
   i2_opts o{};
   if (opts) o = *opts;
+  if (o.loop_mode < I2_LOOP_GRAPH || o.loop_mode > I2_LOOP_RELAUNCH) return I2_ERR_ARG;
   if (algo != I2_CC && !srcs_host && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
   if (algo == I2_SSSP) {
     if (!g->g.eweight) return I2_ERR_ARG;
@@ -931,15 +1041,29 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     }
     I2_CK(cudaMemcpyAsync(g->srcs, srcs_host, sizeof(int) * nsrc, cudaMemcpyHostToDevice, s));
   }
-  const RunParams rp = make_params(g, algo, mode, variant, src, nsrc, o.iter_cap);
+  const int delta = pick_delta(g, algo, mode, variant, o.sssp_delta);
+  if (delta > 0) {
+    st = ensure_piles(g);
+    if (st) return st;
+  }
+  const RunParams rp = make_params(g, algo, mode, variant, src, nsrc, o.iter_cap, delta);
   ExecEntry* ex = nullptr;
-  if (o.loop_mode == I2_LOOP_GRAPH) {
-    st = build_exec(g, algo, mode, variant, multi, rp, &ex);
+  const bool graph_loop = o.loop_mode == I2_LOOP_GRAPH || o.loop_mode == I2_LOOP_RELAUNCH;
+  if (graph_loop) {
+    // Resident traversal where the device takes the cooperative node; graphs
+    // with one launch per iteration otherwise.
+    const bool resident = o.loop_mode == I2_LOOP_GRAPH && g->resident_ok;
+    st = build_exec(g, algo, mode, variant, multi, resident, rp, &ex);
+    if (st && resident) {
+      cudaGetLastError();
+      g->resident_ok = false;
+      st = build_exec(g, algo, mode, variant, multi, false, rp, &ex);
+    }
     if (st) return st;
   }
   double host_relax_ms = -1.0;
   if (rep) I2_CK(cudaEventRecord(g->ev0, s));
-  if (o.loop_mode == I2_LOOP_GRAPH) {
+  if (graph_loop) {
     st = launch_exec(g, ex, rp, s);
     if (st) return st;
   } else {
@@ -951,7 +1075,7 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   if (rep) I2_CK(cudaEventRecord(g->ev1, s));
   I2_CK(cudaGetLastError());
   // Without a report the call stays asynchronous on the stream.
-  if (!rep && o.loop_mode == I2_LOOP_GRAPH) return I2_OK;
+  if (!rep && graph_loop) return I2_OK;
   return fill_report(g, s, algo, rep, host_relax_ms);
 }
 
@@ -1076,6 +1200,7 @@ const char* i2_status_string(int status) {
     case I2_ERR_ITER_CAP: return "iteration cap reached";
     case I2_ERR_OVERFLOW: return "int32 limit exceeded";
     case I2_ERR_CAPACITY: return "graph exceeds the fixed scratch of i2_run_noalloc";
+    case I2_ERR_STALL: return "a resident traversal's barrier wait ran out of time";
   }
   return "unknown status";
 }
@@ -1507,7 +1632,7 @@ extern "C" int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* di
 
   // The scratch keeps the previous call's contents: the bitmaps must start at
   // zero (k_reset rewrites the control block, k_fill the output).
-  RunParams rp;
+  RunParams rp{};
   rp.algo = algo;
   rp.mode = 0;
   rp.fixed_variant = kVPCta;
@@ -1520,7 +1645,7 @@ extern "C" int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* di
   KernelFn ff = fill_kernel(algo);
   ff<<<grid_for(ff, 8), kBlock, 0, s>>>(c);
   seed_kernel(algo)<<<1, kBlock, 0, s>>>(c);
-  KernelFn fn = relax_kernel(algo, kVPCta);
+  KernelFn fn = relax_kernel(algo, kVPCta, false);
   const int grid = grid_for(fn, 8);
   Ctl h;
   for (;;) {

@@ -10,7 +10,7 @@ typedef void (*KernelFn)(Ctx);
 
 int cuda_status(cudaError_t e);
 int grid_for(KernelFn fn, int max_per_sm);
-KernelFn relax_kernel(int algo, int variant);
+KernelFn relax_kernel(int algo, int variant, bool near_far = false);
 const float* mlp_device_params();
 int mlp_install(const float* params, int count);
 

@@ -35,7 +35,10 @@ namespace i2 {
 namespace cg = cooperative_groups;
 
 constexpr int kScanItems = kQueue / kBlock;                 // staged entries per thread in a flush
-constexpr int kEdgesPerThread = 4;                          // edge-balanced variant
+#ifndef I2_EB_EDGES
+#define I2_EB_EDGES 4
+#endif
+constexpr int kEdgesPerThread = I2_EB_EDGES;                // edge-balanced variant
 constexpr int kTileEdges = kBlock * kEdgesPerThread;        // edges per edge-balanced tile
 
 typedef cub::BlockScan<int, kBlock> BlockScanT;
@@ -46,12 +49,14 @@ struct Acc {
   int maxdeg;
   int mindist;
   int visited;
+  int fmin;  // smallest value put on a far pile
 };
 
 __device__ __forceinline__ void acc_init(Acc& a) {
   a.maxdeg = 0;
   a.mindist = kInf;
   a.visited = 0;
+  a.fmin = kInf;
 }
 
 // Per-block staging of pushes into the next frontier.
@@ -90,6 +95,7 @@ __device__ __forceinline__ void acc_reduce(Acc a, S& s) {
     a.maxdeg = max(a.maxdeg, __shfl_down_sync(0xffffffffu, a.maxdeg, o));
     a.mindist = min(a.mindist, __shfl_down_sync(0xffffffffu, a.mindist, o));
     a.visited += __shfl_down_sync(0xffffffffu, a.visited, o);
+    a.fmin = min(a.fmin, __shfl_down_sync(0xffffffffu, a.fmin, o));
   }
   __syncthreads();
   if ((threadIdx.x & 31) == 0) s.red[threadIdx.x >> 5] = a;
@@ -99,6 +105,7 @@ __device__ __forceinline__ void acc_reduce(Acc a, S& s) {
       s.red[0].maxdeg = max(s.red[0].maxdeg, s.red[w].maxdeg);
       s.red[0].mindist = min(s.red[0].mindist, s.red[w].mindist);
       s.red[0].visited += s.red[w].visited;
+      s.red[0].fmin = min(s.red[0].fmin, s.red[w].fmin);
     }
   }
 }
@@ -116,6 +123,33 @@ __device__ __forceinline__ void direct_append(unsigned long long* packed, int* l
   const int pos = (int)(base >> 32) + (int)g.thread_rank();
   list[pos] = v;
   off[pos] = (unsigned)(base & 0xffffffffu) + (unsigned)pre;
+}
+
+// Append v to a far pile; the threads that append together share one atomic.
+__device__ __forceinline__ void pile_append(int* pile, unsigned* size, int v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(size, (unsigned)g.size());
+  base = g.shfl(base, 0);
+  pile[base + g.thread_rank()] = v;
+}
+
+// Defer v (new value val, at or above the threshold) to the current far pile.
+// The pile's bitmap keeps one entry per vertex: a vertex already on the pile
+// only lowers the pile's minimum. Vertices without edges are never deferred.
+__device__ __forceinline__ void defer_vertex(const Ctx& c, Acc& a, int v, int val, int old) {
+  if (old == kInf) a.visited++;
+  a.fmin = min(a.fmin, val);
+  const unsigned bit = 1u << (v & 31);
+  unsigned* w = &c.fbm[v >> 5];
+  if (*(volatile unsigned*)w & bit) return;
+  if (atomicOr(w, bit) & bit) return;
+  if (c.g.nindex[v + 1] == c.g.nindex[v]) {
+    atomicAnd(w, ~bit);
+    return;
+  }
+  const int p = c.ctl->pcur;
+  pile_append(c.pile[p], &c.ctl->psize[p], v);
 }
 
 // Record vertex v (degree deg >= 1) in the next frontier. The bitmap bit is
@@ -316,7 +350,7 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
 }
 
 // Last j in [0, n) with off[j] <= x (off[0] == 0 <= x).
-__device__ __forceinline__ int owner_search(const unsigned* __restrict__ off, int n, unsigned x) {
+__device__ __forceinline__ int owner_search(const unsigned* off, int n, unsigned x) {
   int lo = 0, hi = n;
   while (hi - lo > 1) {
     const int mid = lo + ((hi - lo) >> 1);
@@ -328,7 +362,7 @@ __device__ __forceinline__ int owner_search(const unsigned* __restrict__ off, in
 // Warp-cooperative version for global arrays (warp 0 calls it; every lane gets
 // the result): each round probes 32 evenly spaced positions, so the range
 // shrinks 32-fold per round of parallel loads instead of 2-fold per dependent load.
-__device__ __forceinline__ int owner_search_warp(const unsigned* __restrict__ off, int n, unsigned x) {
+__device__ __forceinline__ int owner_search_warp(const unsigned* off, int n, unsigned x) {
   const int lane = threadIdx.x & 31;
   int lo = 0, hi = n;  // off[lo] <= x, answer in [lo, hi)
   while (hi - lo > 32) {
@@ -372,7 +406,7 @@ __device__ void heavy_path(const Ctx& c, Stage& s, Acc& a, int cur, int nxt, int
   unsigned t0, t1;
   block_share(ntiles, active, &t0, &t1);
   if (t0 >= t1) return;  // uniform
-  const unsigned* __restrict__ toff = c.htoff[cur];
+  const unsigned* toff = c.htoff[cur];
   if (threadIdx.x < 32) {
     const int j = owner_search_warp(toff, nh, t0);
     if (threadIdx.x == 0) s.j0 = j;
@@ -426,7 +460,7 @@ __device__ __forceinline__ int active_blocks(const Ctx& c, int old, long long ne
 // iteration. Every block of the launch, active or not, counts into `done`, so
 // the iteration advances only after every block has read its state.
 template <typename S>
-__device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a, int i, int cur, int nxt, int old,
+__device__ __forceinline__ bool block_epilogue(const Ctx& c, S& s, const Acc& a, int i, int cur, int nxt, int old,
                                                int /*active*/) {
   acc_reduce(a, s);
   if (threadIdx.x == 0) {
@@ -435,32 +469,38 @@ __device__ __forceinline__ void block_epilogue(const Ctx& c, S& s, const Acc& a,
     if (r.maxdeg) atomicMax(&sl.maxdeg, r.maxdeg);
     if (r.mindist != kInf) atomicMin(&sl.mindist, r.mindist);
     if (r.visited) atomicAdd((unsigned long long*)&c.ctl->visited, (unsigned long long)r.visited);
+    // far pushes of a relax launch go onto pile pcur, a split's onto the other
+    if (r.fmin != kInf) atomicMin(&c.ctl->pmin[c.ctl->split ? 1 - c.ctl->pcur : c.ctl->pcur], r.fmin);
     __threadfence();
     const unsigned t = atomicAdd(&c.ctl->done, 1u);
     s.last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (s.last) {
+  const bool last = s.last;
+  if (last) {
     __threadfence();
     finish_iteration(c, i, cur, nxt, old);
   }
+  return last;  // this block finished the iteration
 }
 
 // The launch's start time is taken by block 0, which the scheduler dispatches
 // first; the last block reads it after every block has finished.
 // Epilogue of a block with no work in this launch.
 template <typename S>
-__device__ __forceinline__ void idle_epilogue(const Ctx& c, S& s, int i, int cur, int nxt, int old) {
+__device__ __forceinline__ bool idle_epilogue(const Ctx& c, S& s, int i, int cur, int nxt, int old) {
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned t = atomicAdd(&c.ctl->done, 1u);
     s.last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (s.last) {
+  const bool last = s.last;
+  if (last) {
     __threadfence();
     finish_iteration(c, i, cur, nxt, old);
   }
+  return last;  // this block finished the iteration
 }
 
 __device__ __forceinline__ void block_prologue(const Ctx& c) {
@@ -472,7 +512,7 @@ __device__ __forceinline__ void block_prologue(const Ctx& c) {
 // vertex. Heavy vertices are skipped here and taken by the heavy path.
 
 template <int ALG, int VAR>
-__device__ __forceinline__ void body_push(const Ctx& c, Stage& s) {
+__device__ __forceinline__ bool body_push(const Ctx& c, Stage& s) {
   block_prologue(c);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
@@ -480,15 +520,14 @@ __device__ __forceinline__ void body_push(const Ctx& c, Stage& s) {
   const int per = VAR == kVPThread ? kBlock : (VAR == kVPWarp ? kBlock / kWarp : 1);
   const int active = active_blocks(c, old, ((long long)n + per - 1) / per + slot_edges(c.ctl->slot[cur].hpacked));
   if (blockIdx.x >= active) {
-    idle_epilogue(c, s, i, cur, nxt, old);
-    return;
+    return idle_epilogue(c, s, i, cur, nxt, old);
   }
   stage_init(s);
   Acc a;
   acc_init(a);
   clear_old(c, old, active);
   __syncthreads();
-  const int* __restrict__ wl = c.wl[cur];
+  const int* wl = c.wl[cur];
 
   for (;;) {
     if (threadIdx.x == 0) s.chunk = atomicAdd(&c.ctl->chunk, per);
@@ -523,7 +562,7 @@ __device__ __forceinline__ void body_push(const Ctx& c, Stage& s) {
   }
   heavy_path<ALG>(c, s, a, cur, nxt, active);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old, active);
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -537,7 +576,7 @@ __device__ __forceinline__ void body_push(const Ctx& c, Stage& s) {
 // warp scan and one packed atomic. No vertex is too big or too small: work is
 // split by edges, as in the reference's edge-centric codes.
 constexpr int kWarpTile = kWarp * kEdgesPerThread;  // edges per warp tile
-constexpr int kWarpQueue = 2 * kWarpTile;           // warp staging capacity
+constexpr int kWarpQueue = 256;                    // warp staging capacity (overflow appends directly)
 constexpr int kWarpsPerBlock = kBlock / kWarp;
 
 struct WarpStage {
@@ -562,8 +601,13 @@ __device__ __forceinline__ void warp_stage_entry(const Ctx& c, WarpStage& ws, Ac
   if (deg >= c.heavy) direct_append(&c.ctl->slot[nxt].hpacked, c.hwl[nxt], c.htoff[nxt], v, heavy_tiles(deg));
 }
 
+template <bool DEFER>
 __device__ __forceinline__ void warp_push_vertex(const Ctx& c, WarpStage& ws, Acc& a, int nxt, int v, int val,
-                                                 int old) {
+                                                 int old, int thr) {
+  if (DEFER && val >= thr) {
+    defer_vertex(c, a, v, val, old);
+    return;
+  }
   if (old == kInf) a.visited++;
   a.mindist = min(a.mindist, val);
   const unsigned bit = 1u << (v & 31);
@@ -620,9 +664,9 @@ __device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt)
   __syncwarp();
 }
 
-template <int ALG>
+template <int ALG, bool DEFER>
 __device__ __forceinline__ void warp_relax_batch(const Ctx& c, WarpStage& ws, Acc& a, int nxt, const int* du,
-                                                 const int* nv, const int* wv, const bool* ok) {
+                                                 const int* nv, const int* wv, const bool* ok, int thr) {
   int cand[kEdgesPerThread], cur[kEdgesPerThread];
 #pragma unroll
   for (int r = 0; r < kEdgesPerThread; ++r) {
@@ -633,7 +677,7 @@ __device__ __forceinline__ void warp_relax_batch(const Ctx& c, WarpStage& ws, Ac
   for (int r = 0; r < kEdgesPerThread; ++r) {
     if (cand[r] < cur[r]) {
       const int old = atomicMin(&c.dist[nv[r]], cand[r]);
-      if (cand[r] < old) warp_push_vertex(c, ws, a, nxt, nv[r], cand[r], old);
+      if (cand[r] < old) warp_push_vertex<DEFER>(c, ws, a, nxt, nv[r], cand[r], old, thr);
     }
   }
 }
@@ -644,9 +688,10 @@ struct EpiStage {
 };
 
 // Minimum resident blocks per SM the edge-balanced kernel is compiled for
-// (bounds its registers: 6 -> 40 per thread).
+// (bounds its registers: 5 -> 48 per thread). On RMAT-22, 5 measured 10-13%
+// faster than 4 or 6 for BFS, SSSP and CC; 8 edges per lane was slower.
 #ifndef I2_EB_MIN_BLOCKS
-#define I2_EB_MIN_BLOCKS 6
+#define I2_EB_MIN_BLOCKS 5
 #endif
 
 struct EBShared {
@@ -654,20 +699,21 @@ struct EBShared {
   WarpStage wss[kWarpsPerBlock];
 };
 
-template <int ALG>
-__device__ __forceinline__ void body_edge_balanced(const Ctx& c, EBShared& sh) {
+// Split launch of the SSSP near/far ordering (F_i is empty, the far pile is
+// not, the threshold has just risen from T0 to T). Each pile entry with a
+// distance below T moves into F_{i+1}; one at or above T moves onto the other
+// pile. An entry whose distance is below T0 was lowered after it was deferred
+// by a push that put it into a frontier (values only fall and the threshold
+// only rises), so it has been relaxed with that distance and is dropped.
+__device__ __forceinline__ bool body_split(const Ctx& c, EBShared& sh, int i, int cur, int nxt, int old) {
   EpiStage& s = sh.s;
-  block_prologue(c);
-  const int i = c.ctl->iter;
-  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  const unsigned long long P = c.ctl->slot[cur].packed;
-  const int n = slot_size(P);
-  const unsigned total = slot_edges(P);
-  const int active = active_blocks(c, old, ((long long)total + kWarpTile * kWarpsPerBlock - 1) /
-                                              (kWarpTile * kWarpsPerBlock));
+  Ctl* ctl = c.ctl;
+  const int p = ctl->pcur;
+  const unsigned n = ctl->psize[p];
+  const int T = ctl->threshold, T0 = ctl->prev_threshold;
+  const int active = active_blocks(c, old, ((long long)n + kBlock - 1) / kBlock);
   if (blockIdx.x >= active) {
-    idle_epilogue(c, s, i, cur, nxt, old);
-    return;
+    return idle_epilogue(c, s, i, cur, nxt, old);
   }
   if (threadIdx.x == 0) s.last = 0;
   Acc a;
@@ -677,8 +723,67 @@ __device__ __forceinline__ void body_edge_balanced(const Ctx& c, EBShared& sh) {
   WarpStage& ws = sh.wss[threadIdx.x >> 5];
   if (lane == 0) ws.n = 0;
   __syncwarp();
-  const int* __restrict__ wl = c.wl[cur];
-  const unsigned* __restrict__ woff = c.woff[cur];
+  const int* from = c.pile[p];
+  int* to = c.pile[1 - p];
+  const unsigned stride = (unsigned)active * kBlock;
+  // warp-uniform loop: every lane takes part in the flushes
+  for (unsigned base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += stride) {
+    const unsigned j = base + lane;
+    if (j < n) {
+      const int v = from[j];
+      const unsigned bit = 1u << (v & 31);
+      const int d = c.dist[v];
+      if (d < T) {
+        atomicAnd(&c.fbm[v >> 5], ~bit);
+        if (d >= T0) {
+          atomicOr(&c.bm[nxt][v >> 5], bit);
+          a.mindist = min(a.mindist, d);
+          warp_stage_entry(c, ws, a, nxt, v, c.g.nindex[v + 1] - c.g.nindex[v]);
+        }
+      } else {
+        a.fmin = min(a.fmin, d);
+        pile_append(to, &ctl->psize[1 - p], v);
+      }
+    }
+    __syncwarp();
+    if (ws.n >= kWarpQueue - kWarp) warp_flush(c, ws, nxt);
+  }
+  warp_flush(c, ws, nxt);
+  __syncthreads();
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
+}
+
+// DEFER: SSSP near/far ordering (pushes at or above the threshold go onto the
+// far pile, and split launches refill the frontier from it).
+template <int ALG, bool DEFER = false>
+__device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBShared& sh) {
+  static_assert(!DEFER || ALG == kSSSP, "near/far ordering is for SSSP");
+  EpiStage& s = sh.s;
+  block_prologue(c);
+  const int i = c.ctl->iter;
+  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
+  if (DEFER && c.ctl->split) {
+    return body_split(c, sh, i, cur, nxt, old);
+  }
+  const int thr = DEFER ? c.ctl->threshold : kInf;
+  const unsigned long long P = c.ctl->slot[cur].packed;
+  const int n = slot_size(P);
+  const unsigned total = slot_edges(P);
+  const int active = active_blocks(c, old, ((long long)total + kWarpTile * kWarpsPerBlock - 1) /
+                                              (kWarpTile * kWarpsPerBlock));
+  if (blockIdx.x >= active) {
+    return idle_epilogue(c, s, i, cur, nxt, old);
+  }
+  if (threadIdx.x == 0) s.last = 0;
+  Acc a;
+  acc_init(a);
+  clear_old(c, old, active);
+  const int lane = threadIdx.x & 31;
+  WarpStage& ws = sh.wss[threadIdx.x >> 5];
+  if (lane == 0) ws.n = 0;
+  __syncwarp();
+  const int* wl = c.wl[cur];
+  const unsigned* woff = c.woff[cur];
   const int* __restrict__ nl = c.g.nlist;
   const int* __restrict__ ew = c.g.eweight;
   // Only as many warps as there are warp tiles take part, so a small frontier
@@ -694,20 +799,23 @@ __device__ __forceinline__ void body_edge_balanced(const Ctx& c, EBShared& sh) {
     int j = owner_search_warp(woff, n, W0);  // entry holding edge W0
     for (unsigned e0 = W0; e0 < W1; e0 += kWarpTile) {
       const unsigned e1 = min(W1, e0 + kWarpTile);
-      // offsets of the entries from j on, 32 at a time, until one reaches e1
+      // offsets of the entries from j on, 32 at a time, until one reaches e1;
+      // each batch's vertex ids are loaded with its offsets, and the adjacency
+      // start and value of the entries inside the tile right after
       int m = 0;
       for (;;) {
         const int jj = j + m + lane;
-        const unsigned w = jj < n ? woff[jj] : total;
+        const bool in = jj < n;
+        const unsigned w = in ? woff[jj] : total;
+        const int v = in ? wl[jj] : 0;
         ws.off[m + lane] = w;
         const int below = __popc(__ballot_sync(0xffffffffu, w < e1));
+        if (lane < below) {  // offsets ascend: the entries below e1 are a prefix
+          ws.beg[m + lane] = c.g.nindex[v];
+          ws.du[m + lane] = c.dist[v];
+        }
         m += below;
         if (below < kWarp) break;
-      }
-      for (int k = lane; k < m; k += kWarp) {
-        const int v = wl[j + k];
-        ws.beg[k] = c.g.nindex[v];
-        ws.du[k] = c.dist[v];
       }
       __syncwarp();
       const unsigned x0 = e0 + (unsigned)lane * kEdgesPerThread;
@@ -730,23 +838,23 @@ __device__ __forceinline__ void body_edge_balanced(const Ctx& c, EBShared& sh) {
           ok[r] = Op<ALG>::valid(du[r]);
         }
       }
-      warp_relax_batch<ALG>(c, ws, a, nxt, du, nv, wv, ok);
+      warp_relax_batch<ALG, DEFER>(c, ws, a, nxt, du, nv, wv, ok, thr);
       // the next tile starts at e1: its first entry is the last one with offset <= e1
       j += (ws.off[m] == e1) ? m : m - 1;
       __syncwarp();
-      if (ws.n >= kWarpQueue - kWarpTile) warp_flush(c, ws, nxt);
+      if (ws.n >= kWarpQueue / 2) warp_flush(c, ws, nxt);
     }
   }
   warp_flush(c, ws, nxt);
   __syncthreads();
-  block_epilogue(c, s, a, i, cur, nxt, old, active);
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
 // Bitmap-gated topology sweep: thread per vertex, light vertices only; heavy
 // frontier vertices take the shared heavy path.
 template <int ALG>
-__device__ __forceinline__ void body_push_topo(const Ctx& c, Stage& s) {
+__device__ __forceinline__ bool body_push_topo(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
@@ -756,7 +864,7 @@ __device__ __forceinline__ void body_push_topo(const Ctx& c, Stage& s) {
   const int active = gridDim.x;  // topology sweeps use the whole grid
   clear_old(c, old, active);
   __syncthreads();
-  const unsigned* __restrict__ bmc = c.bm[cur];
+  const unsigned* bmc = c.bm[cur];
   const int V = c.g.nodes;
   for (long long base = (long long)blockIdx.x * kBlock; base < V; base += (long long)gridDim.x * kBlock) {
     const int v = (int)base + threadIdx.x;
@@ -770,13 +878,13 @@ __device__ __forceinline__ void body_push_topo(const Ctx& c, Stage& s) {
   }
   heavy_path<ALG>(c, s, a, cur, nxt, active);
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old, active);
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
 // Edge-centric sweep over all CSR entries, gated by the source's frontier bit.
 template <int ALG>
-__device__ __forceinline__ void body_edge_topo(const Ctx& c, Stage& s) {
+__device__ __forceinline__ bool body_edge_topo(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
@@ -786,7 +894,7 @@ __device__ __forceinline__ void body_edge_topo(const Ctx& c, Stage& s) {
   const int active = gridDim.x;  // topology sweeps use the whole grid
   clear_old(c, old, active);
   __syncthreads();
-  const unsigned* __restrict__ bmc = c.bm[cur];
+  const unsigned* bmc = c.bm[cur];
   const int E = c.g.edges;
   const long long units = ((long long)E + 3) >> 2;
   const int* __restrict__ sp = c.g.sp;
@@ -829,7 +937,7 @@ __device__ __forceinline__ void body_edge_topo(const Ctx& c, Stage& s) {
     stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old, active);
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -838,7 +946,7 @@ __device__ __forceinline__ void body_edge_topo(const Ctx& c, Stage& s) {
 // frontier's bitmap is written with one plain store per warp. dist[v] is only
 // written by v's own thread, so no atomics are needed on it.
 template <int ALG, bool FRONTIER>
-__device__ __forceinline__ void body_pull(const Ctx& c, Stage& s) {
+__device__ __forceinline__ bool body_pull(const Ctx& c, Stage& s) {
   block_prologue(c);
   stage_init(s);
   Acc a;
@@ -848,7 +956,7 @@ __device__ __forceinline__ void body_pull(const Ctx& c, Stage& s) {
   const int active = gridDim.x;  // every vertex is visited
   clear_old(c, old, active);
   __syncthreads();
-  const unsigned* __restrict__ bmc = c.bm[cur];
+  const unsigned* bmc = c.bm[cur];
   const int V = c.g.nodes;
   const int* __restrict__ nl = c.g.nlist;
   const int* __restrict__ ew = c.g.eweight;
@@ -894,7 +1002,7 @@ __device__ __forceinline__ void body_pull(const Ctx& c, Stage& s) {
     stage_flush_if_half(c, s, nxt);
   }
   stage_flush(c, s, nxt);
-  block_epilogue(c, s, a, i, cur, nxt, old, active);
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -913,6 +1021,12 @@ template <int ALG>
 __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(Ctx c) {
   __shared__ EBShared sh;
   body_edge_balanced<ALG>(c, sh);
+}
+
+// Edge-balanced SSSP push with near/far ordering (Ctl::delta > 0).
+__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_near_far(Ctx c) {
+  __shared__ EBShared sh;
+  body_edge_balanced<kSSSP, true>(c, sh);
 }
 
 template <int ALG>
@@ -937,6 +1051,85 @@ union AnyShared {
   Stage st;
   EBShared eb;
 };
+
+// ---------------------------------------------------------------------------
+// Resident traversal: one launch runs the iterations one after another, the
+// grid meeting at a barrier where separate launches would meet at a kernel
+// boundary. The block that finishes an iteration (the last one to count into
+// `done`) has already advanced the control block when it bumps bar_gen, which
+// releases the others. Every wait is bounded by Ctl::stall_ns: a block that
+// waits longer sets kStatusStall and leaves, and every other block leaves at
+// its next wait, so the launch always ends. All blocks must be resident at
+// once, which the cooperative launch attribute of the graph node guarantees.
+// Data written in one iteration is read by other blocks in the next, so the
+// bodies read the frontier lists, bitmaps and values with coherent loads only
+// (the read-only path is used for the graph arrays alone).
+
+// Thread 0 of a block: return once bar_gen has moved past `gen`, or once the
+// wait has run out (status kStatusStall) or another block has given up.
+__device__ __forceinline__ void grid_wait(Ctl* ctl, unsigned gen) {
+  const unsigned long long t0 = globaltimer();
+  const unsigned long long limit = *(volatile unsigned long long*)&ctl->stall_ns;
+  for (unsigned k = 1;; ++k) {
+    if (*(volatile unsigned*)&ctl->bar_gen != gen) break;
+    if (*(volatile int*)&ctl->status & kStatusStall) break;
+    __nanosleep(k < 256 ? 20 : 200);
+    if ((k & 63) == 0 && globaltimer() - t0 > limit) {
+      atomicOr(&ctl->status, kStatusStall);
+      break;
+    }
+  }
+}
+
+template <int ALG, int VAR, bool DEFER>
+__device__ __forceinline__ bool run_body(const Ctx& c, AnyShared& sh) {
+  const int v = VAR >= 0 ? VAR : *(volatile int*)&c.ctl->variant;  // uniform: written before the release
+  switch (v) {
+    case kVPThread: return body_push<ALG, kVPThread>(c, sh.st);
+    case kVPWarp: return body_push<ALG, kVPWarp>(c, sh.st);
+    case kVPCta: return body_edge_balanced<ALG, DEFER>(c, sh.eb);
+    case kVPBlock: return body_push<ALG, kVPBlock>(c, sh.st);
+    case kPullFrontier: return body_pull<ALG, true>(c, sh.st);
+    case kPullTopo: return body_pull<ALG, false>(c, sh.st);
+    case kEdgeTopo: return body_edge_topo<ALG>(c, sh.st);
+    default: return body_push_topo<ALG>(c, sh.st);
+  }
+}
+
+// VAR >= 0: that style every iteration; VAR < 0: the style picked for each
+// iteration by the previous one (heuristic or learned selector).
+template <int ALG, int VAR, bool DEFER = false>
+__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_resident(Ctx c) {
+  __shared__ AnyShared sh;
+  __shared__ int s_go;
+  Ctl* ctl = c.ctl;
+  if (threadIdx.x == 0) s_go = !(*(volatile int*)&ctl->status & kStatusStall);
+  __syncthreads();
+  if (!s_go) {  // an earlier launch of this traversal gave up: end the graph's loop
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c.use_loop)
+      cudaGraphSetConditional((cudaGraphConditionalHandle)c.loop_h, 0u);
+    return;
+  }
+  unsigned gen = *(volatile unsigned*)&ctl->bar_gen;  // no iteration ends before every block arrives
+  bool first = true;
+  for (;;) {
+    const bool last = run_body<ALG, VAR, DEFER>(c, sh);
+    if (threadIdx.x == 0) {
+      if (last && !(first && *(volatile int*)&ctl->hold)) {
+        __threadfence();
+        atomicAdd(&ctl->bar_gen, 1u);
+      } else {
+        grid_wait(ctl, gen);
+      }
+      __threadfence();
+      s_go = *(volatile int*)&ctl->go && !(*(volatile int*)&ctl->status & kStatusStall);
+    }
+    first = false;
+    ++gen;
+    __syncthreads();
+    if (!s_go) break;
+  }
+}
 
 template <int ALG>
 __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_dispatch(Ctx c) {

@@ -20,7 +20,7 @@ def test_iteration_cap_is_a_status(gpu):
             nl.append(v + 1)
     g = i2.ECLGraph(n, len(nl), nindex, np.array(nl, np.int32), np.ones(len(nl), np.int32))
     dg = i2.DeviceGraph.upload(g)
-    for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+    for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
         with pytest.raises(i2.I2Error) as e:
             dg.bfs(0, iter_cap=3, loop=loop)
         assert e.value.status == _capi.I2_ERR_ITER_CAP
@@ -89,3 +89,39 @@ def test_wrap_refuses_host_pointers(gpu):
     assert e.value.status == _capi.I2_ERR_ARG
     ok = i2.DeviceGraph.wrap_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr())
     ok.free()
+
+
+def test_resident_barrier_wait_is_bounded(gpu, monkeypatch):
+    # The resident loop's blocks meet at a barrier between iterations. With
+    # the first release withheld (a release that nothing gives), every block's
+    # wait must run out after the stall limit and the run must end with
+    # I2_ERR_STALL, leaving the context usable.
+    import time
+
+    g = i2.gen_er(5000, 20000, 4)
+    dg = i2.DeviceGraph.upload(g)
+    ref, _ = dg.bfs(0, loop=i2.I2_LOOP_HOST)
+    monkeypatch.setenv("I2_TEST_HOLD_BARRIER", "1")
+    monkeypatch.setenv("I2_STALL_MS", "300")
+    for variant in ("vp_cta", "heuristic"):
+        t0 = time.perf_counter()
+        with pytest.raises(i2.I2Error) as e:
+            dg.bfs(0, variant=variant)
+        dt = time.perf_counter() - t0
+        assert e.value.status == _capi.I2_ERR_STALL
+        assert 0.25 < dt < 10.0
+    monkeypatch.delenv("I2_TEST_HOLD_BARRIER")
+    monkeypatch.delenv("I2_STALL_MS")
+    for variant in ("vp_cta", "heuristic"):
+        d, _ = dg.bfs(0, variant=variant)
+        np.testing.assert_array_equal(d, ref)
+    dg.free()
+
+
+def test_bad_loop_mode_is_refused(gpu):
+    g = i2.gen_er(100, 300, 2)
+    dg = i2.DeviceGraph.upload(g)
+    with pytest.raises(i2.I2Error) as e:
+        dg.bfs(0, loop=3)
+    assert e.value.status == _capi.I2_ERR_ARG
+    dg.free()

@@ -34,7 +34,7 @@ def test_golden_all_variants_both_loops(gpu, golden):
         dg = i2.DeviceGraph.upload(case["graph"])
         assert dg.info["symmetric"] == 1, name
         for v in _variants_for(dg):
-            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
                 for s in case["sources"]:
                     d, _ = dg.bfs(s, variant=v, loop=loop)
                     np.testing.assert_array_equal(d, case["bfs"][s], err_msg=f"{name} bfs {v} {loop} {s}")
@@ -66,13 +66,14 @@ def test_seeded_all_variants_vs_oracle(gpu, seeded, name):
     src = int(np.argmax(g.degrees()))
     ref_b, ref_s, ref_c = oracle.bfs(g, src), oracle.sssp(g, src), oracle.cc(g)
     for v in _variants_for(dg):
-        d, rep = dg.bfs(src, variant=v)
-        np.testing.assert_array_equal(d, ref_b, err_msg=f"bfs {v}")
-        assert rep.reached_vertices == int((ref_b != i2.INF).sum())
-        d, _ = dg.sssp(src, variant=v)
-        np.testing.assert_array_equal(d, ref_s, err_msg=f"sssp {v}")
-        lab, _ = dg.cc(variant=v)
-        np.testing.assert_array_equal(lab, ref_c, err_msg=f"cc {v}")
+        for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_RELAUNCH):
+            d, rep = dg.bfs(src, variant=v, loop=loop)
+            np.testing.assert_array_equal(d, ref_b, err_msg=f"bfs {v} {loop}")
+            assert rep.reached_vertices == int((ref_b != i2.INF).sum())
+            d, _ = dg.sssp(src, variant=v, loop=loop)
+            np.testing.assert_array_equal(d, ref_s, err_msg=f"sssp {v} {loop}")
+            lab, _ = dg.cc(variant=v, loop=loop)
+            np.testing.assert_array_equal(lab, ref_c, err_msg=f"cc {v} {loop}")
     dg.free()
 
 
@@ -185,4 +186,70 @@ def test_reference_interface_mirror(gpu, golden):
     for fn in (i2.GPUcc_vertex, i2.GPUcc_edge):
         fn(dg, out)
         np.testing.assert_array_equal(out, case["cc"])
+    dg.free()
+
+
+def _directed_chain():
+    # 0 -> 1 -> 2 -> 3 (3 has no out-edges), 4 -> 2, heavy first hop
+    return i2.ECLGraph(5, 4, np.array([0, 1, 2, 3, 3, 4], np.int32), np.array([1, 2, 3, 2], np.int32),
+                       np.array([300, 1, 4, 2], np.int32))
+
+
+@pytest.mark.parametrize("name", ["er", "rmat14", "grid", "rmat16", "directed", "unit"])
+def test_sssp_near_far_ordering_any_step(gpu, seeded, name):
+    # Near/far ordering defers pushes at or above a rising threshold; the
+    # distances must not depend on the step, including steps far below and far
+    # above every weight, on graphs with vertices that have no out-edges.
+    if name == "directed":
+        g = _directed_chain()
+    elif name == "unit":
+        g0 = seeded["rmat14"]
+        g = i2.ECLGraph(g0.nodes, g0.edges, g0.nindex, g0.nlist, np.ones(g0.edges, np.int32))
+    else:
+        g = seeded[name]
+    dg = i2.DeviceGraph.upload(g)
+    deg = g.degrees()
+    srcs = [0, int(np.argmax(deg))]
+    if name == "directed":
+        srcs = [0, 4]
+    for s in srcs:
+        ref = oracle.sssp(g, s)
+        for delta in (-1, 0, 1, 3, 100, 5000, 1 << 20, 1 << 30):
+            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+                d, rep = dg.sssp(s, variant="vp_cta", loop=loop, delta=delta)
+                np.testing.assert_array_equal(d, ref, err_msg=f"{name} src {s} delta {delta} loop {loop}")
+                assert rep.reached_vertices == int((ref != i2.INF).sum())
+    dg.free()
+
+
+def test_sssp_near_far_golden_and_repeat(gpu, golden):
+    for name, case in golden.items():
+        dg = i2.DeviceGraph.upload(case["graph"])
+        for s in case["sources"]:
+            for delta in (0, 1, 64, 1 << 16):
+                for _ in range(2):  # the piles' state must not leak into the next run
+                    d, _ = dg.sssp(s, variant="vp_cta", delta=delta)
+                    np.testing.assert_array_equal(d, case["sssp"][s], err_msg=f"{name} {s} {delta}")
+        dg.free()
+
+
+def test_sssp_near_far_reduces_relaxed_work(gpu, seeded):
+    # The point of the ordering: fewer vertices are relaxed more than once.
+    # With a step of a few mean weights over the mean degree the per-iteration
+    # records must show fewer frontier edges in total than plain
+    # frontier-driven relaxation, which is also what delta <= 0 runs. (How
+    # many edges plain relaxation scans depends on the order of the atomics,
+    # so the comparison is a bound, not an equality.)
+    g = seeded["rmat16"]
+    dg = i2.DeviceGraph.upload(g)
+    src = int(np.argmax(g.degrees()))
+    base = []
+    for delta in (-1, 0):
+        _, rep = dg.sssp(src, variant="vp_cta", delta=delta, record=True)
+        base.append((rep.iterations, sum(r["edges"] for r in dg.records())))
+    step = max(1, int(round(4 * g.eweight.mean() / g.degrees().mean())))
+    _, rep = dg.sssp(src, variant="vp_cta", delta=step, record=True)
+    near_far = sum(r["edges"] for r in dg.records())
+    assert near_far < 0.8 * min(b[1] for b in base)
+    assert rep.iterations > max(b[0] for b in base)
     dg.free()
