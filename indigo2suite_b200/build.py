@@ -20,6 +20,7 @@ LIB = PKG / "libi2b200.so"
 
 SOURCES = [
     "engine.cu",
+    "resident.cu",
     "selector.cu",
     "batch.cu",
     "gen_device.cu",

@@ -5,11 +5,14 @@
 // (k_fill, k_seed), then one relax launch per iteration until the frontier is
 // empty (the do-while of the reference's host drivers, e.g.
 // BFS_CUDA_V_Data_Push_..._Warp_..._NonDup.cu:112-122). In the default loop
-// mode the whole sequence is one CUDA graph: a WHILE conditional node whose
-// body is one kernel, either the fixed style's relax kernel or the dispatch
-// kernel whose blocks branch on the style picked for this iteration. The relax
-// kernels' last block picks the next style and sets the loop condition on the
-// device, so there is no host round trip per iteration.
+// mode (I2_LOOP_GRAPH) the whole sequence is one CUDA graph whose WHILE
+// conditional node holds one cooperative relax launch that runs every
+// iteration itself, its blocks meeting at a bounded barrier between
+// iterations (relax_resident, resident.cu). I2_LOOP_RELAUNCH keeps one launch
+// per iteration inside the graph: the fixed style's kernel, or the dispatch
+// kernel whose blocks branch on the style picked for this iteration. Either
+// way the last block of an iteration picks the next style and sets the loop
+// condition on the device, so there is no host round trip per iteration.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -25,149 +28,12 @@
 #include "host_graph.h"
 #include "mlp.cuh"
 #include "relax.cuh"
+#include "iteration.cuh"
 
 namespace i2 {
 
 static_assert(sizeof(IterRec) == sizeof(i2_iter_record), "record layout");
 static_assert((int)kNumVariants == (int)I2_NUM_VARIANTS, "variant count");
-
-// ---------------------------------------------------------------------------
-// Selection of the next variant.
-
-// Fixed frontier-size rule: bottom-up pull for BFS levels whose frontier
-// carries more than 1/16 of the edges (direction-optimising BFS), otherwise the
-// edge-balanced push, which measured fastest of the push styles on every
-// family tried.
-__device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, unsigned long long edges) {
-  (void)size;
-  const float fe = (float)edges;
-  const float E = (float)gs.edges;
-  auto ok = [&](int v) { return (allowed >> v) & 1; };
-  if (algo == kBFS && ok(kPullFrontier) && fe > E * (1.f / 16.f)) return kPullFrontier;
-  return ok(kVPCta) ? kVPCta : kVPThread;
-}
-
-// Executed by every thread of one block. Computes the features of the frontier
-// in slot `nxt`, picks the variant for the next launch and sets the loop
-// condition of the graph. `cond` tells whether another launch will happen.
-// The learned selector is re-evaluated when the frontier's entries or edges
-// moved by more than a factor 1.5 since its last evaluation, or 16 iterations
-// passed; otherwise the previous choice stands (long tails of small, similar
-// frontiers do not pay for an inference each).
-__device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
-  __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], y[kOut];
-  __shared__ int s_eval;
-  Ctl* ctl = c.ctl;
-  if (threadIdx.x == 0) {
-    volatile Slot* sl = &ctl->slot[nxt];
-    const unsigned long long p = sl->packed;
-    const int n = slot_size(p);
-    const unsigned e = slot_edges(p);
-    frontier_features(c.gs, ctl->algo, next_iter, n, slot_size(sl->hpacked), e, sl->maxdeg,
-                      *(volatile long long*)&ctl->visited, x);
-    for (int k = 0; k < kFeatures; ++k) ctl->feat[k] = x[k];
-    const long long sn = ctl->sel_n, se = ctl->sel_e;
-    s_eval = next_iter == 0 || 2LL * n > 3LL * sn || 3LL * n < 2LL * sn || 2LL * e > 3LL * se ||
-             3LL * e < 2LL * se || next_iter - ctl->sel_iter >= 16;
-  }
-  __syncthreads();
-  const int mode = ctl->mode;
-  const bool infer = mode == 2 && c.mlp && cond && s_eval;
-  if (infer) mlp_forward_block(c.mlp, x, h1, h2, y);
-  if (threadIdx.x == 0) {
-    int v = ctl->fixed_variant;
-    if (mode == 1 || (mode == 2 && !c.mlp)) {
-      volatile Slot* sl = &ctl->slot[nxt];
-      const unsigned long long p = sl->packed;
-      v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, slot_size(p), slot_edges(p));
-    } else if (mode == 2) {
-      v = ctl->variant;
-      if (infer) {
-        float best = 3.0e38f;
-        int bv = -1;
-        for (int k = 0; k < kOut; ++k)
-          if (((ctl->allowed >> k) & 1) && y[k] < best) {
-            best = y[k];
-            bv = k;
-          }
-        v = bv < 0 ? kVPCta : bv;
-        volatile Slot* sl = &ctl->slot[nxt];
-        const unsigned long long p = sl->packed;
-        ctl->sel_n = slot_size(p);
-        ctl->sel_e = slot_edges(p);
-        ctl->sel_iter = next_iter;
-      }
-    }
-    ctl->variant = v;
-    if (cond) ctl->hist[v] += 1;
-    ctl->go = cond ? 1 : 0;
-    if (c.use_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)c.loop_h, cond ? 1u : 0u);
-  }
-}
-
-// Last block of a relax launch: record the launch, advance the iteration and
-// decide whether the loop continues.
-__device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old) {
-  __shared__ int s_cond;
-  Ctl* ctl = c.ctl;
-  if (threadIdx.x == 0) {
-    const unsigned long long t1 = globaltimer();
-    const unsigned long long dt = t1 - ctl->tstart;
-    ctl->relax_ns += dt;
-    volatile Slot* sc = &ctl->slot[cur];
-    if (c.recs && i < c.rec_cap) {
-      IterRec& r = c.recs[i];
-      r.iter = i;
-      r.variant = ctl->variant;
-      r.size = slot_size(sc->packed);
-      r.hsize = slot_size(sc->hpacked);
-      r.edges = slot_edges(sc->packed);
-      r.maxdeg = sc->maxdeg;
-      r.mindist = sc->mindist;
-      r.visited = *(volatile long long*)&ctl->visited;
-      r.t_ns = dt;
-      for (int k = 0; k < kFeatures; ++k) r.feat[k] = ctl->feat[k];
-    }
-    Slot& so = ctl->slot[old];
-    so.packed = 0;
-    so.hpacked = 0;
-    so.maxdeg = 0;
-    so.mindist = kInf;
-    ctl->done = 0;
-    ctl->chunk = 0;
-    ctl->htile = 0;
-    ctl->tstart = ~0ull;
-    ctl->iter = i + 1;
-    volatile Slot* sn = &ctl->slot[nxt];
-    const long long n = slot_size(sn->packed);
-    int cond = n > 0;
-    if (ctl->delta > 0) {
-      if (ctl->split) {  // this launch emptied pile pcur onto the other one
-        const int p = ctl->pcur;
-        ctl->psize[p] = 0;
-        ctl->pmin[p] = kInf;
-        ctl->pcur = 1 - p;
-        ctl->split = 0;
-      }
-      const int p = ctl->pcur;
-      if (n == 0 && *(volatile unsigned*)&ctl->psize[p] > 0) {
-        // next launch splits the pile at a raised threshold
-        const long long lo = max((long long)ctl->threshold, (long long)*(volatile int*)&ctl->pmin[p]);
-        ctl->prev_threshold = ctl->threshold;
-        ctl->threshold = (int)min(lo + (long long)ctl->delta, (long long)kInf);
-        ctl->split = 1;
-        cond = 1;
-      }
-    }
-    if (cond && i + 1 >= ctl->iter_cap) {
-      ctl->status |= kStatusIterCap;
-      cond = 0;
-    }
-    s_cond = cond;
-  }
-  __syncthreads();
-  select_next(c, i + 1, nxt, s_cond != 0);
-}
 
 // ---------------------------------------------------------------------------
 // Init kernels.
@@ -429,30 +295,6 @@ static KernelFn dispatch_kernel(int algo) {
   if (algo == kBFS) return relax_dispatch<kBFS>;
   if (algo == kSSSP) return relax_dispatch<kSSSP>;
   return relax_dispatch<kCC>;
-}
-
-template <int ALG>
-static KernelFn resident_fn(int v) {
-  switch (v) {
-    case kVPThread: return relax_resident<ALG, kVPThread>;
-    case kVPWarp: return relax_resident<ALG, kVPWarp>;
-    case kVPCta: return relax_resident<ALG, kVPCta>;
-    case kVPBlock: return relax_resident<ALG, kVPBlock>;
-    case kPullFrontier: return relax_resident<ALG, kPullFrontier>;
-    case kPullTopo: return relax_resident<ALG, kPullTopo>;
-    case kEdgeTopo: return relax_resident<ALG, kEdgeTopo>;
-    case kPushTopo: return relax_resident<ALG, kPushTopo>;
-  }
-  return relax_resident<ALG, -1>;  // per-iteration pick
-}
-
-// Kernel of a resident traversal: fixed style v (mode 0) or the per-iteration
-// pick (v < 0).
-static KernelFn resident_kernel(int algo, int v, bool near_far) {
-  if (near_far && algo == kSSSP && v == kVPCta) return relax_resident<kSSSP, kVPCta, true>;
-  if (algo == kBFS) return resident_fn<kBFS>(v);
-  if (algo == kSSSP) return resident_fn<kSSSP>(v);
-  return resident_fn<kCC>(v);
 }
 
 KernelFn relax_kernel(int algo, int v, bool near_far) {

@@ -43,6 +43,24 @@ constexpr int kTileEdges = kBlock * kEdgesPerThread;        // edges per edge-ba
 
 typedef cub::BlockScan<int, kBlock> BlockScanT;
 
+// Loads of the graph's adjacency (nlist, eweight, sp): each entry is read
+// about once per iteration, so it is loaded with an evict-first policy, which
+// keeps the randomly accessed, L2-sized arrays (values, bitmaps, frontier
+// lists, nindex) resident in L2 instead of the streamed lines. On RMAT-22 this
+// measured 3-7% faster for BFS, SSSP and CC than the read-only path.
+// I2_STREAM_LOADS: 0 read-only path without a hint, 1 evict-first (default).
+#ifndef I2_STREAM_LOADS
+#define I2_STREAM_LOADS 1
+#endif
+template <typename T>
+__device__ __forceinline__ T ld_adj(const T* p) {
+#if I2_STREAM_LOADS
+  return __ldcs(p);
+#else
+  return __ldg(p);
+#endif
+}
+
 // Frontier statistics of one thread's pushes; kept in registers and reduced
 // once per block at the end of the launch.
 struct Acc {
@@ -314,10 +332,10 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
       int nv[4], wv[4] = {0, 0, 0, 0};
       bool ok[4];
       if (k0 + 3 < c.g.edges) {
-        const int4 x = __ldg(reinterpret_cast<const int4*>(nl + k0));
+        const int4 x = ld_adj(reinterpret_cast<const int4*>(nl + k0));
         nv[0] = x.x; nv[1] = x.y; nv[2] = x.z; nv[3] = x.w;
         if (Op<ALG>::kWeighted) {
-          const int4 y = __ldg(reinterpret_cast<const int4*>(ew + k0));
+          const int4 y = ld_adj(reinterpret_cast<const int4*>(ew + k0));
           wv[0] = y.x; wv[1] = y.y; wv[2] = y.z; wv[3] = y.w;
         }
 #pragma unroll
@@ -341,8 +359,8 @@ __device__ __forceinline__ void relax_range(const Ctx& c, Stage& s, Acc& a, int 
       for (int r = 0; r < 4; ++r) {
         const long long k = k0 + r;
         ok[r] = k < hi;
-        nv[r] = ok[r] ? __ldg(nl + k) : 0;
-        if (Op<ALG>::kWeighted) wv[r] = ok[r] ? __ldg(ew + k) : 0;
+        nv[r] = ok[r] ? ld_adj(nl + k) : 0;
+        if (Op<ALG>::kWeighted) wv[r] = ok[r] ? ld_adj(ew + k) : 0;
       }
       relax_batch<ALG, 4>(c, s, a, nxt, dus, nv, wv, ok);
     }
@@ -441,7 +459,7 @@ __device__ __forceinline__ void clear_old(const Ctx& c, int old, int active) {
   }
 }
 
-__device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old);
+static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old);
 
 // Blocks of a launch that take part in it. Blocks at or above this index
 // return at once, so a small frontier does not pay for the whole grid; the
@@ -832,8 +850,8 @@ __device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBShared& sh) {
         if (ok[r]) {
           while (x >= ws.off[o + 1]) ++o;
           const int e = ws.beg[o] + (int)(x - ws.off[o]);
-          nv[r] = __ldg(nl + e);
-          if (Op<ALG>::kWeighted) wv[r] = __ldg(ew + e);
+          nv[r] = ld_adj(nl + e);
+          if (Op<ALG>::kWeighted) wv[r] = ld_adj(ew + e);
           du[r] = ws.du[o];
           ok[r] = Op<ALG>::valid(du[r]);
         }
@@ -907,12 +925,12 @@ __device__ __forceinline__ bool body_edge_topo(const Ctx& c, Stage& s) {
       int su[4], nv[4], wv[4] = {0, 0, 0, 0}, du[4];
       bool ok[4];
       if (c.g.vec_ok && k0 + 3 < E) {
-        const int4 x = __ldg(reinterpret_cast<const int4*>(sp + k0));
+        const int4 x = ld_adj(reinterpret_cast<const int4*>(sp + k0));
         su[0] = x.x; su[1] = x.y; su[2] = x.z; su[3] = x.w;
-        const int4 y = __ldg(reinterpret_cast<const int4*>(nl + k0));
+        const int4 y = ld_adj(reinterpret_cast<const int4*>(nl + k0));
         nv[0] = y.x; nv[1] = y.y; nv[2] = y.z; nv[3] = y.w;
         if (Op<ALG>::kWeighted) {
-          const int4 z = __ldg(reinterpret_cast<const int4*>(ew + k0));
+          const int4 z = ld_adj(reinterpret_cast<const int4*>(ew + k0));
           wv[0] = z.x; wv[1] = z.y; wv[2] = z.z; wv[3] = z.w;
         }
       } else {
@@ -975,11 +993,11 @@ __device__ __forceinline__ bool body_pull(const Ctx& c, Stage& s) {
         const int end = c.g.nindex[v + 1];
         deg = end - beg;
         for (int k = beg; k < end; ++k) {
-          const int u = __ldg(nl + k);
+          const int u = ld_adj(nl + k);
           if (FRONTIER && !((bmc[u >> 5] >> (u & 31)) & 1u)) continue;
           const int du = c.dist[u];
           if (!Op<ALG>::valid(du)) continue;
-          const int cd = Op<ALG>::cand(du, Op<ALG>::kWeighted ? __ldg(ew + k) : 0);
+          const int cd = Op<ALG>::cand(du, Op<ALG>::kWeighted ? ld_adj(ew + k) : 0);
           if (cd < best) {
             best = cd;
             if (FRONTIER && best == bound) break;
@@ -1024,7 +1042,7 @@ __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(
 }
 
 // Edge-balanced SSSP push with near/far ordering (Ctl::delta > 0).
-__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_near_far(Ctx c) {
+static __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_near_far(Ctx c) {
   __shared__ EBShared sh;
   body_edge_balanced<kSSSP, true>(c, sh);
 }
