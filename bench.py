@@ -179,6 +179,27 @@ def ref_cpu_baseline(g, src: int, runs: int, name: str) -> dict:
             "program": name, "sample": f"full workload graph, {runs} traversals, median of the reference's own timer"}
 
 
+def ref_cuda_baseline(g, src: int) -> dict:
+    """The reference's own CUDA SSSP in the benchmark's style (E_Data_Push, S1:
+    codes/cuda/sssp-cuda/SSSP_CUDA_E_Data_Push_..._NonDup.cu, built unchanged for
+    sm_100a in oracle/_ref) on the same graph file, timed by its own main."""
+    import tempfile
+
+    import oracle
+
+    if not (oracle.REF_OUT / "cuda_sssp_edge_s1").exists():
+        return {"unavailable": "oracle/_ref/cuda_sssp_edge_s1 not built"}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.egr")
+        oracle.write_egr(g, path)
+        r = oracle.run_ref_program("cuda_sssp_edge_s1", [path, str(src), "0"], timeout=900)
+    if r["rc"] != 0 or not r["runtime"]:
+        return {"unavailable": f"S1 exited {r['rc']}: {r['out'][-200:]}"}
+    return {"program": "cuda_sssp_edge_s1 (reference S1, E_Data_Push, sm_100a)", "runtime_s": r["runtime"],
+            "value": 1e-9 * g.edges / r["runtime"], "unit": UNIT,
+            "sample": "full workload graph; the program's own runtime print (device loop, verification off)"}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -356,6 +377,12 @@ def run_ours(args, rank: int, world: int, local: int):
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
+    ref_cuda = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_cuda = ref_cuda_baseline(host, src)
+        except Exception as exc:  # reported, not fatal
+            ref_cuda = {"unavailable": str(exc)}
 
     # per step: k_reset, k_fill, k_seed and the relax launch(es)
     launches = args.steps * (3 + (1 if graph_loop else rep_g.iterations))
@@ -364,7 +391,8 @@ def run_ours(args, rank: int, world: int, local: int):
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}",
                            loop=args.loop, near_far_step=delta if delta > 0 else "off"),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_query": e2e_query,
+            "roofline": roofline, "cpu_baseline": cpu, "reference_cuda": ref_cuda, "e2e": e2e,
+            "e2e_query": e2e_query,
             "gpu_launches": launches, "clocks": clk,
             "styles_gteps": styles, "best_fixed_style": max(fixed, key=fixed.get),
             "iterations": rep_g.iterations, "reached_vertices": rep_g.reached_vertices,
@@ -385,6 +413,69 @@ def _event_time(torch, stream, fn, steps: int) -> float:
     e1.record(stream)
     e1.synchronize()
     return e0.elapsed_time(e1) * 1e-3 / steps
+
+
+def run_er16(args, rank: int, world: int, local: int):
+    """Config: ER G(n=65,536, m=262,144 distinct undirected pairs) = 524,288 CSR
+    entries, BFS from vertex 0 -- the reference's CPU configuration. Our GPU
+    BFS (fixed edge-balanced style and the heuristic), beside the reference's
+    OpenMP and C++-threads BFS programs on this host at all cores and at one.
+    Replicas only: each rank runs the same traversal."""
+    import torch
+
+    import indigo2suite_b200 as i2
+    import oracle
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    g = i2.gen_er(65536, 262144, 1)
+    if g.edges != 524288:
+        raise SystemExit(f"ER graph has {g.edges} CSR entries, expected 524288")
+    dg = i2.DeviceGraph.upload(g)
+    ref = oracle.bfs(g, 0)
+    res = {}
+    for v in ("vp_cta", "heuristic"):
+        d, _ = dg.bfs(0, variant=v)
+        if not np.array_equal(d, ref):
+            raise SystemExit(f"BFS {v} differs from the oracle")
+        run = lambda: dg.run_device(i2.I2_BFS, 0, variant=v, stream=sp, report=False)  # noqa: E731
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        res[v] = _event_time(torch, stream, run, args.steps)
+    dist.barrier()
+    t = dist.max(res["vp_cta"], dev)
+    cpu = {}
+    if rank == 0 and not args.no_cpu_baseline:
+        nproc = os.cpu_count() or 1
+        for prog in ("bfs_omp", "bfs_cpp"):
+            for th in (nproc, 1):
+                ts = []
+                for _ in range(3):
+                    tt, out = oracle.ref_cpu_run(prog, g, 0, th)
+                    ts.append(tt)
+                if not np.array_equal(out, ref):
+                    raise SystemExit(f"reference {prog} result differs from the oracle")
+                cpu[f"{prog}_{th}t"] = {"value": 1e-9 * g.edges / statistics.median(ts), "unit": UNIT,
+                                        "cores": th, "seconds": statistics.median(ts)}
+    best = max(cpu.values(), key=lambda x: x["value"]) if cpu else None
+    line = {"metric": METRIC, "value": world * 1e-9 * g.edges / t, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "er16_bfs_cpu_config", "nodes": g.nodes, "edges": g.edges, "source": 0,
+                       "variant": "vp_cta", "l2": "graph fits in L2 (2.4 MB): launch-latency bound",
+                       "parallelism": f"replicas x{world}"},
+            "heuristic_gteps": world * 1e-9 * g.edges / dist.max(res["heuristic"], dev),
+            "cpu_baseline": (dict(best, kind="reference", sample="full graph, median of 3 of the program's own timer",
+                                  all=cpu) if best else None),
+            "verified": "bit-exact vs the oracle (GPU and reference CPU programs)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dg.free()
+    dist.close()
 
 
 def run_batch512(args, rank: int, world: int, local: int):
@@ -571,7 +662,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-styles", action="store_true", help="skip the per-style comparison")
-    ap.add_argument("--workload", choices=["sssp_rmat22", "batch512", "grid4096", "rmat26"], default="sssp_rmat22",
+    ap.add_argument("--workload", choices=["sssp_rmat22", "batch512", "grid4096", "rmat26", "er16"],
+                    default="sssp_rmat22",
                     help="sssp_rmat22 is the benchmark line; the others are the other configurations")
     ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
                     help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
@@ -585,7 +677,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    {"sssp_rmat22": run_ours, "batch512": run_batch512, "grid4096": run_grid4096,
+    {"sssp_rmat22": run_ours, "batch512": run_batch512, "grid4096": run_grid4096, "er16": run_er16,
      "rmat26": run_rmat26}[args.workload](args, rank, world, local)
 
 
