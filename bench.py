@@ -323,6 +323,8 @@ def run_ours(args, rank: int, world: int, local: int):
         name = v if isinstance(v, str) else i2.VARIANTS[v]
         if v in (4, 5) and not dg.info["symmetric"]:
             continue
+        if v == 8:  # union-find computes CC labels only
+            continue
         with torch.cuda.stream(stream):
             steps(1, v)
         f0 = torch.cuda.Event(enable_timing=True)
@@ -579,6 +581,8 @@ def run_grid4096(args, rank: int, world: int, local: int):
         res = {}
         for v in list(range(i2.I2_NUM_VARIANTS)) + ["heuristic", "learned"]:
             name = v if isinstance(v, str) else i2.VARIANTS[v]
+            if v == 8 and algo != i2.I2_CC:  # union-find computes CC labels only
+                continue
             run = lambda: dg.run_device(algo, 0, variant=v, stream=sp, report=False)  # noqa: E731
             run()
             torch.cuda.synchronize()
@@ -627,7 +631,14 @@ def run_rmat26(args, rank: int, world: int, local: int):
     lo, hi = shard.shard_range(64, rank, world)
     mine = srcs[lo:hi]
     res = {}
+    peak, peak_kind = peaks()
     for an, algo in (("bfs", i2.I2_BFS), ("sssp", i2.I2_SSSP), ("cc", i2.I2_CC)):
+        # algorithmic bytes per traversal (reached counts of the first source:
+        # every source with an edge lies in the giant component)
+        rep = dg.run_device(algo, mine[0], variant="vp_cta", stream=sp)
+        b_alg = {"bfs": 8.0 * rep.reached_edges + 20.0 * rep.reached_vertices,
+                 "sssp": 12.0 * rep.reached_edges + 20.0 * rep.reached_vertices,
+                 "cc": 8.0 * dg.edges + 12.0 * dg.nodes}[an]
         for v in ("vp_cta", "heuristic", "learned"):
             ss = mine if algo != i2.I2_CC else mine[:1]
             dg.run_device(algo, ss[0], variant=v, stream=sp, report=False)
@@ -636,12 +647,15 @@ def run_rmat26(args, rank: int, world: int, local: int):
             t = _event_time(torch, stream, lambda: dg.run_device(algo, next(it), variant=v, stream=sp, report=False),
                             len(ss))
             t = dist.max(t, dev)
-            res[f"{an}/{v}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t}
+            res[f"{an}/{v}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t,
+                                "b_alg_gb": 1e-9 * b_alg, "achieved_gbs": 1e-9 * b_alg / t,
+                                "roofline_frac": 1e-9 * b_alg / t / peak}
     line = {"metric": METRIC, "value": world * res["bfs/learned"]["gteps"], "unit": UNIT, "n_gpus": world,
             "steps": 64, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": "rmat26_bfs_sssp_cc_64src", "nodes": dg.nodes, "edges": dg.edges,
                        "generation_s": gen_s, "parallelism": f"sources sharded x{world}"},
+            "roofline_peak_gbs": peak, "roofline_peak_source": peak_kind,
             "results": res}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -66,7 +66,10 @@ enum {
   I2_PULL_TOPO = 5,       /* topology-driven pull from all neighbours; symmetric graphs */
   I2_EDGE_TOPO = 6,       /* edge-centric sweep over all CSR entries */
   I2_PUSH_TOPO = 7,       /* topology sweep of the frontier bitmap, thread per vertex */
-  I2_NUM_VARIANTS = 8
+  I2_UNION_FIND = 8,      /* CC on symmetric graphs only: union-find over all edges, linking the
+                             larger root below the smaller, then every label set to its root
+                             (two launches; same minimum-ID labels as label propagation) */
+  I2_NUM_VARIANTS = 9
 };
 
 /* Loop modes. */
@@ -90,6 +93,10 @@ typedef struct {
                        pile until the near frontier is empty). <= 0: off
                        (plain frontier-driven relaxation), > 0: this step.
                        The distances do not depend on it. */
+  int then_at;      /* > 0: run `variant` for iterations 0..then_at-1 and then_variant
+                       from iteration then_at on (a fixed switch of style; results do
+                       not change). 0: no switch. */
+  int then_variant;
 } i2_opts;
 
 typedef struct {

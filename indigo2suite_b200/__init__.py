@@ -175,10 +175,13 @@ class Report:
     status: int = 0
 
 
-def _opts(variant, loop, iter_cap, record, stream, delta: int = 0) -> capi.Opts:
-    """delta: SSSP near/far threshold step for the vp_cta style (<= 0 off, > 0 this step)."""
+def _opts(variant, loop, iter_cap, record, stream, delta: int = 0, then_variant=None, then_at: int = 0) -> capi.Opts:
+    """delta: SSSP near/far threshold step for the vp_cta style (<= 0 off, > 0 this step).
+    then_variant/then_at: switch to then_variant from iteration then_at on."""
+    tv = variant_id(then_variant) if then_variant is not None else 0
     return capi.Opts(variant_id(variant), int(loop), int(iter_cap), int(record),
-                     C.c_void_p(stream) if stream else None, int(delta))
+                     C.c_void_p(stream) if stream else None, int(delta), int(then_at) if then_variant is not None else 0,
+                     tv)
 
 
 def _report(r: capi.Report, status: int) -> Report:
@@ -257,10 +260,11 @@ class DeviceGraph:
             pass
 
     # -- traversals ---------------------------------------------------------
-    def _run(self, algo: int, src: int, variant, loop, iter_cap, record, stream, out=None, delta=0):
+    def _run(self, algo: int, src: int, variant, loop, iter_cap, record, stream, out=None, delta=0,
+             then_variant=None, then_at=0):
         dist = out if out is not None else np.empty(self.nodes, np.int32)
         assert dist.dtype == np.int32 and dist.size >= self.nodes and dist.flags.c_contiguous
-        o = _opts(variant, loop, iter_cap, record, stream, delta)
+        o = _opts(variant, loop, iter_cap, record, stream, delta, then_variant, then_at)
         r = capi.Report()
         if algo == I2_BFS:
             st = lib.i2_bfs(self._h, src, _iptr(dist), C.byref(o), C.byref(r))
@@ -272,15 +276,17 @@ class DeviceGraph:
             raise I2Error(st, ["bfs", "sssp", "cc"][algo])
         return dist, _report(r, st)
 
-    def bfs(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
-        return self._run(I2_BFS, src, variant, loop, iter_cap, record, stream, out)
+    def bfs(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
+            then_variant=None, then_at: int = 0):
+        return self._run(I2_BFS, src, variant, loop, iter_cap, record, stream, out, 0, then_variant, then_at)
 
     def sssp(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
-             delta: int = 0):
-        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out, delta)
+             delta: int = 0, then_variant=None, then_at: int = 0):
+        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out, delta, then_variant, then_at)
 
-    def cc(self, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
-        return self._run(I2_CC, 0, variant, loop, iter_cap, record, stream, out)
+    def cc(self, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
+           then_variant=None, then_at: int = 0):
+        return self._run(I2_CC, 0, variant, loop, iter_cap, record, stream, out, 0, then_variant, then_at)
 
     def run_device(self, algo: int, src: int = 0, out_ptr: int = 0, variant="vp_cta", loop=I2_LOOP_GRAPH,
                    iter_cap=0, record=False, stream=None, report: bool = True, delta: int = 0) -> Report | None:

@@ -30,7 +30,8 @@ I2_BFS, I2_SSSP, I2_CC = 0, 1, 2
 
 I2_AUTO_HEURISTIC = -1
 I2_AUTO_LEARNED = -2
-VARIANTS = ["vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo", "edge_topo", "push_topo"]
+VARIANTS = ["vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo", "edge_topo", "push_topo",
+            "union_find"]
 I2_NUM_VARIANTS = len(VARIANTS)
 I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH = 0, 1, 2
 
@@ -44,7 +45,8 @@ class EclGraphC(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("variant", C.c_int), ("loop_mode", C.c_int), ("iter_cap", C.c_int),
-                ("record_iters", C.c_int), ("stream", C.c_void_p), ("sssp_delta", C.c_int)]
+                ("record_iters", C.c_int), ("stream", C.c_void_p), ("sssp_delta", C.c_int),
+                ("then_at", C.c_int), ("then_variant", C.c_int)]
 
 
 class Report(C.Structure):

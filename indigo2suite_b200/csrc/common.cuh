@@ -54,7 +54,8 @@ enum Variant {
   kPullTopo = 5,     // topology-driven pull over all vertices and all neighbours
   kEdgeTopo = 6,     // edge-centric sweep over all CSR entries gated by the bitmap
   kPushTopo = 7,     // topology sweep of the frontier bitmap, thread per vertex
-  kNumVariants = 8
+  kUnionFind = 8,    // CC only: union-find over all edges (hook launch, then compress launch)
+  kNumVariants = 9
 };
 
 // Device view of a CSR graph in the ECLgraph layout (include/ECLgraph.h:44-50).
@@ -109,7 +110,7 @@ struct Ctl {
   unsigned long long tstart;// earliest block start of the current launch (globaltimer ns)
   long long visited;        // vertices reached so far
   int hist[kMaxVariants];   // launches per variant
-  int mode;                 // 0 fixed, 1 heuristic, 2 learned
+  int mode;                 // 0 fixed, 1 heuristic, 2 learned, 3 fixed switch (then_at)
   int fixed_variant;
   int allowed;              // bitmask of variants allowed on this graph
   int src;                  // source vertex (BFS/SSSP)
@@ -131,6 +132,10 @@ struct Ctl {
   int pcur;
   unsigned psize[2];
   int pmin[2];              // lower bound of the values on each pile
+  int uf_phase;             // union-find CC: 1 after the hook launch (the compress launch follows)
+  int then_at;              // mode 3: iteration from which then_variant runs
+  int then_variant;
+  int pad2;
   // Resident launches (one launch runs every iteration, the grid meeting at
   // a barrier between them).
   unsigned bar_gen;         // barrier generation, bumped once per iteration

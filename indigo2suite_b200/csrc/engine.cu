@@ -110,13 +110,13 @@ __global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
   }
   __threadfence();
   __syncthreads();
-  select_next(c, 0, 0, true);
+  select_next(c, 0, 0, true, -1);
 }
 
 // Per-run parameters, passed by value to k_reset so that queued runs never
 // share a host buffer.
 struct RunParams {
-  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap, delta, hold, stall_ms;
+  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap, delta, hold, stall_ms, then_at, then_variant;
   bool operator!=(const RunParams& o) const { return std::memcmp(this, &o, sizeof(RunParams)) != 0; }
 };
 
@@ -135,6 +135,8 @@ __global__ void k_reset(Ctl* ctl, RunParams p) {
   ctl->nsrc = p.nsrc;
   ctl->algo = p.algo;
   ctl->delta = p.delta;
+  ctl->then_at = p.then_at;
+  ctl->then_variant = p.then_variant;
   ctl->hold = p.hold;
   ctl->stall_ns = (unsigned long long)p.stall_ms * 1000000ull;
   ctl->threshold = p.delta > 0 ? p.delta : kInf;  // sources start at 0
@@ -287,6 +289,9 @@ static KernelFn relax_fn(int v) {
     case kPullTopo: return relax_pull<ALG, false>;
     case kEdgeTopo: return relax_edge_topo<ALG>;
     case kPushTopo: return relax_push_topo<ALG>;
+    case kUnionFind:
+      if constexpr (ALG == kCC) return relax_union<ALG>;
+      return nullptr;
   }
   return nullptr;
 }
@@ -598,11 +603,15 @@ static int ensure_symmetry(i2_graph* g) {
   return I2_OK;
 }
 
-static int allowed_mask(const i2_graph* g) {
+// Styles applicable to this graph and algorithm: pull and union-find read a
+// vertex's out-list as its in-list (symmetric graphs only), the edge sweeps
+// need sp[], and union-find computes CC labels only.
+static int allowed_mask(const i2_graph* g, int algo) {
   int m = 0;
   for (int v = 0; v < kNumVariants; ++v) m |= 1 << v;
-  if (g->gs.symmetric != 1) m &= ~((1 << kPullFrontier) | (1 << kPullTopo));
-  if (!g->d_sp) m &= ~(1 << kEdgeTopo);
+  if (g->gs.symmetric != 1) m &= ~((1 << kPullFrontier) | (1 << kPullTopo) | (1 << kUnionFind));
+  if (!g->d_sp) m &= ~((1 << kEdgeTopo) | (1 << kUnionFind));
+  if (algo != I2_CC) m &= ~(1 << kUnionFind);
   return m;
 }
 
@@ -649,7 +658,7 @@ static RunParams make_params(const i2_graph* g, int algo, int mode, int variant,
   p.algo = algo;
   p.mode = mode;
   p.fixed_variant = variant < 0 ? 0 : variant;
-  p.allowed = allowed_mask(g);
+  p.allowed = allowed_mask(g, algo);
   p.src = src;
   p.nsrc = nsrc;
   p.delta = delta;
@@ -797,9 +806,9 @@ static int run_host_loop(i2_graph* g, cudaStream_t s, int algo, bool multi, doub
   for (;;) {
     I2_CK(cudaMemcpyAsync(h, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     I2_CK(cudaStreamSynchronize(s));
-    const int cur = h->iter % 3;
-    const long long n = slot_size(h->slot[cur].packed);
-    if ((n == 0 && !h->split) || (h->status & kStatusIterCap)) break;
+    // the last launch's decision: another frontier, a near/far split, the
+    // compress launch of union-find, or the end (including the iteration cap)
+    if (!h->go || (h->status & kStatusIterCap)) break;
     KernelFn fn = relax_kernel(algo, h->variant, h->delta > 0);
     I2_CK(cudaEventRecord(g->ev2, s));
     fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
@@ -858,15 +867,21 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   if (variant == I2_AUTO_HEURISTIC) mode = 1;
   else if (variant == I2_AUTO_LEARNED) mode = 2;
   else if (variant < 0 || variant >= kNumVariants) return I2_ERR_ARG;
-  if (mode != 0 || variant == kEdgeTopo) {
+  if (o.then_at < 0) return I2_ERR_ARG;
+  if (o.then_at > 0) {  // a fixed switch of style: per-iteration dispatch
+    if (mode != 0 || o.then_variant < 0 || o.then_variant >= kNumVariants) return I2_ERR_ARG;
+    mode = 3;
+  }
+  if (mode != 0 || variant == kEdgeTopo || variant == kUnionFind) {
     st = ensure_sp(g);
     if (st) return st;
   }
-  if (mode != 0 || variant == kPullFrontier || variant == kPullTopo) {
+  if (mode != 0 || variant == kPullFrontier || variant == kPullTopo || variant == kUnionFind) {
     st = ensure_symmetry(g);
     if (st) return st;
   }
-  if (mode == 0 && !((allowed_mask(g) >> variant) & 1)) return I2_ERR_UNSUPPORTED;
+  if ((mode == 0 || mode == 3) && !((allowed_mask(g, algo) >> variant) & 1)) return I2_ERR_UNSUPPORTED;
+  if (mode == 3 && !((allowed_mask(g, algo) >> o.then_variant) & 1)) return I2_ERR_UNSUPPORTED;
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
   const bool multi = srcs_host != nullptr;
   if (multi) {
@@ -888,7 +903,11 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     st = ensure_piles(g);
     if (st) return st;
   }
-  const RunParams rp = make_params(g, algo, mode, variant, src, nsrc, o.iter_cap, delta);
+  RunParams rp = make_params(g, algo, mode, variant, src, nsrc, o.iter_cap, delta);
+  if (mode == 3) {
+    rp.then_at = o.then_at;
+    rp.then_variant = o.then_variant;
+  }
   ExecEntry* ex = nullptr;
   const bool graph_loop = o.loop_mode == I2_LOOP_GRAPH || o.loop_mode == I2_LOOP_RELAUNCH;
   if (graph_loop) {
@@ -972,20 +991,24 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
   KernelFn ff = fill_kernel(algo);
   ff<<<grid_for(ff, 8), kBlock, 0, s>>>(c);
   seed_kernel(algo)<<<1, kBlock, 0, s>>>(c);
-  const int allowed = allowed_mask(g);
+  const int allowed = allowed_mask(g, algo);
   Ctl snap;
   int it = 0;
-  for (; it < cap; ++it) {
+  // Styles are timed through the dispatch kernel, the one the selectors run.
+  KernelFn dk = dispatch_kernel(algo);
+  const int dgrid = grid_for(dk, g->blocks_per_sm);
+  while (it < cap) {
     I2_CK(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     I2_CK(cudaStreamSynchronize(s));
     snap = *g->h_ctl;
-    const int cur = snap.iter % 3;
-    if (slot_size(snap.slot[cur].packed) == 0) break;
+    if (!snap.go || (snap.status & kStatusIterCap)) break;
+    if (snap.uf_phase) {  // the trajectory took union-find: its compress launch is not a choice
+      dk<<<dgrid, kBlock, 0, s>>>(c);
+      I2_CK(cudaGetLastError());
+      continue;
+    }
     I2_CK(cudaMemcpyAsync(g->snap_dist, g->dist, sizeof(int) * V, cudaMemcpyDeviceToDevice, s));
     I2_CK(cudaMemcpyAsync(g->snap_bm, g->bm[0], sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
-    // Styles are timed through the dispatch kernel, the one the selectors run.
-    KernelFn dk = dispatch_kernel(algo);
-    const int dgrid = grid_for(dk, g->blocks_per_sm);
     for (int v = 0; v < kNumVariants; ++v) {
       float best = -1.f;
       if ((allowed >> v) & 1) {
@@ -997,6 +1020,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
           I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
           I2_CK(cudaEventRecord(g->ev0, s));
           dk<<<dgrid, kBlock, 0, s>>>(c);
+          if (v == kUnionFind) dk<<<dgrid, kBlock, 0, s>>>(c);  // its compress launch belongs to it
           I2_CK(cudaEventRecord(g->ev1, s));
           I2_CK(cudaEventSynchronize(g->ev1));
           float ms = 0.f;
@@ -1015,6 +1039,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
     I2_CK(cudaGetLastError());
     if (snap.iter < g->rec_cap)
       I2_CK(cudaMemcpyAsync(&recs[it], g->recs + snap.iter, sizeof(IterRec), cudaMemcpyDeviceToHost, s));
+    ++it;
   }
   I2_CK(cudaStreamSynchronize(s));
   *nout = it;
@@ -1049,7 +1074,7 @@ const char* i2_status_string(int status) {
 
 const char* i2_variant_name(int v) {
   static const char* names[] = {"vp_thread", "vp_warp", "vp_cta", "vp_block",
-                                "pull_frontier", "pull_topo", "edge_topo", "push_topo"};
+                                "pull_frontier", "pull_topo", "edge_topo", "push_topo", "union_find"};
   if (v == I2_AUTO_HEURISTIC) return "auto_heuristic";
   if (v == I2_AUTO_LEARNED) return "auto_learned";
   if (v < 0 || v >= kNumVariants) return "invalid";
@@ -1338,7 +1363,7 @@ int i2_sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_recor
   if (follow >= 0) {
     int st = ensure_symmetry(g);
     if (st) return st;
-    if (!((allowed_mask(g) >> follow) & 1)) return I2_ERR_UNSUPPORTED;
+    if (!((allowed_mask(g, algo) >> follow) & 1)) return I2_ERR_UNSUPPORTED;
   }
   return sweep(g, algo, src, follow, reps, recs, times, cap, n);
 }

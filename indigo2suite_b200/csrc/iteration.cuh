@@ -11,7 +11,10 @@ namespace i2 {
 // ---------------------------------------------------------------------------
 // Selection of the next variant.
 
-// Fixed frontier-size rule: bottom-up pull for BFS levels whose frontier
+// Fixed frontier-size rule: union-find for CC on symmetric graphs of mean
+// degree below 6 (grid-like, high diameter: label propagation needs hundreds
+// of iterations there, while on RMAT and ER graphs it converges in a handful
+// and union-find measured 2-4x slower), bottom-up pull for BFS levels whose frontier
 // carries more than 1/16 of the edges (direction-optimising BFS), otherwise the
 // edge-balanced push, which measured fastest of the push styles on every
 // family tried.
@@ -20,18 +23,20 @@ static __device__ int heuristic_pick(const GStats& gs, int algo, int allowed, in
   const float fe = (float)edges;
   const float E = (float)gs.edges;
   auto ok = [&](int v) { return (allowed >> v) & 1; };
+  if (algo == kCC && ok(kUnionFind) && gs.avgdeg < 6.f) return kUnionFind;
   if (algo == kBFS && ok(kPullFrontier) && fe > E * (1.f / 16.f)) return kPullFrontier;
   return ok(kVPCta) ? kVPCta : kVPThread;
 }
 
 // Executed by every thread of one block. Computes the features of the frontier
 // in slot `nxt`, picks the variant for the next launch and sets the loop
-// condition of the graph. `cond` tells whether another launch will happen.
+// condition of the graph. `cond` tells whether another launch will happen;
+// `force` >= 0 overrides the pick (the compress launch of union-find CC).
 // The learned selector is re-evaluated when the frontier's entries or edges
 // moved by more than a factor 1.5 since its last evaluation, or 16 iterations
 // passed; otherwise the previous choice stands (long tails of small, similar
 // frontiers do not pay for an inference each).
-static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond) {
+static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond, int force) {
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], y[kOut];
   __shared__ int s_eval;
   Ctl* ctl = c.ctl;
@@ -49,11 +54,13 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
   }
   __syncthreads();
   const int mode = ctl->mode;
-  const bool infer = mode == 2 && c.mlp && cond && s_eval;
+  const bool infer = mode == 2 && c.mlp && cond && s_eval && force < 0;
   if (infer) mlp_forward_block(c.mlp, x, h1, h2, y);
   if (threadIdx.x == 0) {
     int v = ctl->fixed_variant;
-    if (mode == 1 || (mode == 2 && !c.mlp)) {
+    if (mode == 3) {
+      v = next_iter >= ctl->then_at ? ctl->then_variant : ctl->fixed_variant;
+    } else if (mode == 1 || (mode == 2 && !c.mlp)) {
       volatile Slot* sl = &ctl->slot[nxt];
       const unsigned long long p = sl->packed;
       v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, slot_size(p), slot_edges(p));
@@ -75,6 +82,7 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
         ctl->sel_iter = next_iter;
       }
     }
+    if (force >= 0) v = force;
     ctl->variant = v;
     if (cond) ctl->hist[v] += 1;
     ctl->go = cond ? 1 : 0;
@@ -85,7 +93,7 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
 // Last block of a relax launch: record the launch, advance the iteration and
 // decide whether the loop continues.
 static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old) {
-  __shared__ int s_cond;
+  __shared__ int s_cond, s_force;
   Ctl* ctl = c.ctl;
   if (threadIdx.x == 0) {
     const unsigned long long t1 = globaltimer();
@@ -136,14 +144,25 @@ static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, i
         cond = 1;
       }
     }
+    int force = -1;
+    if (ctl->variant == kUnionFind) {
+      if (ctl->uf_phase == 0) {  // hook launch done: the compress launch follows
+        ctl->uf_phase = 1;
+        force = kUnionFind;
+        cond = 1;
+      } else {
+        ctl->uf_phase = 0;  // labels final; nothing was pushed
+      }
+    }
     if (cond && i + 1 >= ctl->iter_cap) {
       ctl->status |= kStatusIterCap;
       cond = 0;
     }
     s_cond = cond;
+    s_force = force;
   }
   __syncthreads();
-  select_next(c, i + 1, nxt, s_cond != 0);
+  select_next(c, i + 1, nxt, s_cond != 0, s_force);
 }
 
 }  // namespace i2

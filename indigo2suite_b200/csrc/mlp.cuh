@@ -1,7 +1,7 @@
 // Learned style selector: layout of the MLP parameter blob, the feature vector,
 // and the block-level inference routine used inside the relax kernels' epilogue.
 //
-// Network: x (16 features) -> standardise with (mu, sd) -> 64 ReLU -> 64 ReLU -> 8
+// Network: x (16 features) -> standardise with (mu, sd) -> 64 ReLU -> 64 ReLU -> 9
 // outputs, one predicted log2 launch time (ns) per variant. The selector picks
 // the allowed variant with the smallest prediction. Weights are stored
 // [in][out] so that, for a fixed input, consecutive outputs are consecutive in memory.
@@ -10,7 +10,7 @@
 
 namespace i2 {
 
-static_assert(kBlock == 4 * 64 && kNumVariants * 32 <= kBlock, "mlp_forward_block assumes 256 threads");
+static_assert(kBlock == 4 * 64, "mlp_forward_block assumes 256 threads");
 
 constexpr int kOut = kNumVariants;
 constexpr int kOffMu = 0;
@@ -88,9 +88,8 @@ __device__ __forceinline__ void mlp_forward_block(const float* __restrict__ P, c
     if (q == 0) h2[j] = fmaxf(acc + P[kOffB2 + j], 0.f);
   }
   __syncthreads();
-  const int o = t >> 5;  // output of this warp
   const int lane = t & 31;
-  if (o < kOut) {
+  for (int o = t >> 5; o < kOut; o += kBlock / kWarp) {  // one warp per output
     float acc = 0.f;
 #pragma unroll
     for (int i = 0; i < kHidden / 32; ++i) {

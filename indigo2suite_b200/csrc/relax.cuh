@@ -1029,6 +1029,102 @@ __device__ __forceinline__ bool body_pull(const Ctx& c, Stage& s) {
 // chosen at the end of the previous iteration (one kernel node per iteration
 // instead of a conditional SWITCH node).
 
+// ---------------------------------------------------------------------------
+// Union-find CC (kUnionFind; CC on symmetric graphs only). The labels are read
+// as parent pointers: every label is a vertex of the same component with an ID
+// no larger than the vertex's own (true of the initial labels and of every
+// label propagation writes), so following labels ends at a vertex that is its
+// own label, a root. The hook launch links, for every edge, the roots of its
+// two ends, always the larger root below the smaller one with a compare-and-
+// swap on the larger (which succeeds only while it is still a root). The
+// smallest ID of a component is therefore never linked and ends as the root of
+// the whole component; the compress launch sets every label to its root. The
+// result is the minimum-ID labelling that label propagation converges to,
+// reached from any propagation state in two launches.
+
+// Root of x. With `halve`, each step also points the visited vertex at its
+// grandparent (path halving): any ancestor is a valid label, and a vertex that
+// is not a root never becomes one again, so these plain writes cannot undo a
+// link. Loads are coherent (other threads link and halve concurrently).
+template <bool HALVE>
+__device__ __forceinline__ int uf_find(int* p, int x) {
+  for (;;) {
+    const int px = *(volatile int*)&p[x];
+    if (px == x) return x;
+    const int ppx = *(volatile int*)&p[px];
+    if (HALVE && ppx != px) *(volatile int*)&p[x] = ppx;
+    x = ppx;
+  }
+}
+
+__device__ __forceinline__ void uf_union(int* p, int a, int b) {
+  int ra = uf_find<true>(p, a), rb = uf_find<true>(p, b);
+  while (ra != rb) {
+    if (ra < rb) {
+      const int t = ra;
+      ra = rb;
+      rb = t;
+    }
+    const int seen = atomicCAS(&p[ra], ra, rb);  // link the larger root below the smaller
+    if (seen == ra) return;
+    ra = uf_find<true>(p, seen);  // ra was linked meanwhile: continue from its root
+    rb = uf_find<true>(p, rb);
+  }
+}
+
+template <int ALG>
+__device__ __forceinline__ bool body_union(const Ctx& c, Stage& s) {
+  block_prologue(c);
+  stage_init(s);
+  Acc a;
+  acc_init(a);
+  const int i = c.ctl->iter;
+  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
+  const int active = gridDim.x;
+  clear_old(c, old, active);
+  int* p = c.dist;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (c.ctl->uf_phase == 0) {
+    // hook: every CSR entry (u, v) with v < u, four per thread, 128-bit loads
+    const int E = c.g.edges;
+    const long long units = ((long long)E + 3) >> 2;
+    const int* __restrict__ sp = c.g.sp;
+    const int* __restrict__ nl = c.g.nlist;
+    for (long long q = tid; q < units; q += stride) {
+      const long long k0 = q << 2;
+      int su[4], nv[4];
+      if (c.g.vec_ok && k0 + 3 < E) {
+        const int4 x = ld_adj(reinterpret_cast<const int4*>(sp + k0));
+        const int4 y = ld_adj(reinterpret_cast<const int4*>(nl + k0));
+        su[0] = x.x; su[1] = x.y; su[2] = x.z; su[3] = x.w;
+        nv[0] = y.x; nv[1] = y.y; nv[2] = y.z; nv[3] = y.w;
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const long long k = k0 + r;
+          su[r] = k < E ? sp[k] : 0;
+          nv[r] = k < E ? nl[k] : 0;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (nv[r] < su[r]) uf_union(p, su[r], nv[r]);
+    }
+  } else {
+    // compress: read-only finds (a halving write could replace a finished
+    // label with an intermediate ancestor), each thread writing its own labels
+    const int V = c.g.nodes;
+    for (long long v = tid; v < V; v += stride) {
+      const int r = uf_find<false>(p, (int)v);
+      if (r != (int)v) p[v] = r;
+    }
+  }
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel wrappers.
 template <int ALG, int VAR>
 __global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
   __shared__ Stage s;
@@ -1057,6 +1153,12 @@ template <int ALG>
 __global__ void __launch_bounds__(kBlock) relax_edge_topo(Ctx c) {
   __shared__ Stage s;
   body_edge_topo<ALG>(c, s);
+}
+
+template <int ALG>
+__global__ void __launch_bounds__(kBlock) relax_union(Ctx c) {
+  __shared__ Stage s;
+  body_union<ALG>(c, s);
 }
 
 template <int ALG, bool FRONTIER>
@@ -1110,6 +1212,9 @@ __device__ __forceinline__ bool run_body(const Ctx& c, AnyShared& sh) {
     case kPullFrontier: return body_pull<ALG, true>(c, sh.st);
     case kPullTopo: return body_pull<ALG, false>(c, sh.st);
     case kEdgeTopo: return body_edge_topo<ALG>(c, sh.st);
+    case kUnionFind:
+      if constexpr (ALG == kCC) return body_union<ALG>(c, sh.st);
+      [[fallthrough]];  // not allowed for BFS/SSSP
     default: return body_push_topo<ALG>(c, sh.st);
   }
 }
@@ -1160,6 +1265,12 @@ __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_dispatch(Ctx c
     case kPullFrontier: body_pull<ALG, true>(c, sh.st); break;
     case kPullTopo: body_pull<ALG, false>(c, sh.st); break;
     case kEdgeTopo: body_edge_topo<ALG>(c, sh.st); break;
+    case kUnionFind:
+      if constexpr (ALG == kCC) {
+        body_union<ALG>(c, sh.st);
+        break;
+      }
+      [[fallthrough]];  // not allowed for BFS/SSSP
     default: body_push_topo<ALG>(c, sh.st); break;
   }
 }

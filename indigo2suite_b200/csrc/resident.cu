@@ -20,6 +20,9 @@ static KernelFn resident_fn(int v) {
     case kPullTopo: return relax_resident<ALG, kPullTopo>;
     case kEdgeTopo: return relax_resident<ALG, kEdgeTopo>;
     case kPushTopo: return relax_resident<ALG, kPushTopo>;
+    case kUnionFind:
+      if constexpr (ALG == kCC) return relax_resident<ALG, kUnionFind>;
+      return nullptr;
   }
   return relax_resident<ALG, -1>;  // per-iteration pick
 }

@@ -1,7 +1,7 @@
 // Training and batched inference of the learned style selector (mlp.cuh).
 //
 // Loss: masked mean squared error between predicted and measured log2 launch
-// times, L = sum(M * (Y - T)^2) / sum(M), over rows of 16 features and 8
+// times, L = sum(M * (Y - T)^2) / sum(M), over rows of 16 features and 9
 // per-variant targets. The forward and backward passes are one fused kernel:
 // each block owns kRows rows, keeps the weights and the activations in shared
 // memory, and writes its partial gradient to its own slot; a second kernel sums

@@ -137,7 +137,9 @@ def evaluate(params, specs, algos=("bfs", "sssp", "cc"), log=print) -> list[dict
             algo = ALGOS[an]
             fixed = {}
             for v in range(I2_NUM_VARIANTS):
-                if v in (4, 5) and not sym:
+                if v in (4, 5, 8) and not sym:
+                    continue
+                if v == 8 and an != "cc":  # union-find computes CC labels only
                     continue
                 fixed[VARIANTS[v]] = _time_runs(dg, algo, src, v)
             heur = _time_runs(dg, algo, src, I2_AUTO_HEURISTIC)

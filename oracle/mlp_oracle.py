@@ -8,7 +8,7 @@ Parameter blob layout (float32), identical to the engine's:
   mu[16], sd[16]                     input standardisation (not trained)
   W1[16][64], b1[64]                 weights stored [in][out]
   W2[64][64], b2[64]
-  W3[64][8],  b3[8]
+  W3[64][9],  b3[9]                  one output per variant
 Forward: x_s = (x - mu) / sd; h1 = relu(x_s W1 + b1); h2 = relu(h1 W2 + b2);
 y = h2 W3 + b3 (predicted log2 launch time per variant).
 Loss: sum(M * (y - T)^2) / sum(M).
@@ -17,7 +17,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F, H, O = 16, 64, 8
+F, H, O = 16, 64, 9
 OFF_MU = 0
 OFF_SD = OFF_MU + F
 OFF_W1 = OFF_SD + F

@@ -132,7 +132,7 @@ def test_status_and_variant_names():
     assert i2.lib.i2_status_string(0) == b"ok"
     assert b"iteration cap" in i2.lib.i2_status_string(_capi.I2_ERR_ITER_CAP)
     assert [i2.lib.i2_variant_name(k).decode() for k in range(i2.I2_NUM_VARIANTS)] == i2.VARIANTS
-    assert i2.mlp_param_count() == 16 * 2 + 16 * 64 + 64 + 64 * 64 + 64 + 64 * 8 + 8
+    assert i2.mlp_param_count() == 16 * 2 + 16 * 64 + 64 + 64 * 64 + 64 + 64 * 9 + 9
 
 
 def test_upload_without_device_is_a_status_not_a_crash():

@@ -23,10 +23,15 @@ def _selector_params():
 def _variants_for(dg):
     out = []
     for v in ALL:
-        if v in (4, 5) and not dg.info["symmetric"]:
+        if v in (4, 5, 8) and not dg.info["symmetric"]:
             continue
         out.append(v)
     return out
+
+
+def _for(algo, v):
+    """Union-find (style 8) computes CC labels only."""
+    return v != 8 or algo == "cc"
 
 
 def test_golden_all_variants_both_loops(gpu, golden):
@@ -35,7 +40,7 @@ def test_golden_all_variants_both_loops(gpu, golden):
         assert dg.info["symmetric"] == 1, name
         for v in _variants_for(dg):
             for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
-                for s in case["sources"]:
+                for s in case["sources"] if _for("bfs", v) else []:
                     d, _ = dg.bfs(s, variant=v, loop=loop)
                     np.testing.assert_array_equal(d, case["bfs"][s], err_msg=f"{name} bfs {v} {loop} {s}")
                     d, _ = dg.sssp(s, variant=v, loop=loop)
@@ -67,11 +72,12 @@ def test_seeded_all_variants_vs_oracle(gpu, seeded, name):
     ref_b, ref_s, ref_c = oracle.bfs(g, src), oracle.sssp(g, src), oracle.cc(g)
     for v in _variants_for(dg):
         for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_RELAUNCH):
-            d, rep = dg.bfs(src, variant=v, loop=loop)
-            np.testing.assert_array_equal(d, ref_b, err_msg=f"bfs {v} {loop}")
-            assert rep.reached_vertices == int((ref_b != i2.INF).sum())
-            d, _ = dg.sssp(src, variant=v, loop=loop)
-            np.testing.assert_array_equal(d, ref_s, err_msg=f"sssp {v} {loop}")
+            if _for("bfs", v):
+                d, rep = dg.bfs(src, variant=v, loop=loop)
+                np.testing.assert_array_equal(d, ref_b, err_msg=f"bfs {v} {loop}")
+                assert rep.reached_vertices == int((ref_b != i2.INF).sum())
+                d, _ = dg.sssp(src, variant=v, loop=loop)
+                np.testing.assert_array_equal(d, ref_s, err_msg=f"sssp {v} {loop}")
             lab, _ = dg.cc(variant=v, loop=loop)
             np.testing.assert_array_equal(lab, ref_c, err_msg=f"cc {v} {loop}")
     dg.free()
@@ -139,6 +145,9 @@ def test_directed_graph_push_variants_and_pull_refused(gpu):
         with pytest.raises(i2.I2Error) as e:
             dg.bfs(0, variant=v)
         assert e.value.status == i2._capi.I2_ERR_UNSUPPORTED
+    with pytest.raises(i2.I2Error) as e:  # union-find needs a symmetric graph
+        dg.cc(variant="union_find")
+    assert e.value.status == i2._capi.I2_ERR_UNSUPPORTED
     dg.free()
 
 
@@ -148,8 +157,9 @@ def test_single_vertex_and_edgeless_graphs(gpu):
     for g in (g1, g2):
         dg = i2.DeviceGraph.upload(g)
         for v in ALL:
-            np.testing.assert_array_equal(dg.bfs(0, variant=v)[0], oracle.bfs(g, 0))
-            np.testing.assert_array_equal(dg.sssp(0, variant=v)[0], oracle.sssp(g, 0))
+            if _for("bfs", v):
+                np.testing.assert_array_equal(dg.bfs(0, variant=v)[0], oracle.bfs(g, 0))
+                np.testing.assert_array_equal(dg.sssp(0, variant=v)[0], oracle.sssp(g, 0))
             np.testing.assert_array_equal(dg.cc(variant=v)[0], np.arange(g.nodes))
         dg.free()
 
@@ -252,4 +262,45 @@ def test_sssp_near_far_reduces_relaxed_work(gpu, seeded):
     near_far = sum(r["edges"] for r in dg.records())
     assert near_far < 0.8 * min(b[1] for b in base)
     assert rep.iterations > max(b[0] for b in base)
+    dg.free()
+
+
+def test_union_find_cc(gpu, seeded, golden):
+    # Union-find CC reaches the minimum-ID labels from the initial labels and,
+    # switched to mid-traversal by a selector, from any label-propagation
+    # state; it is refused for BFS and SSSP.
+    for name, g in list(seeded.items()) + [(k, c["graph"]) for k, c in golden.items()]:
+        dg = i2.DeviceGraph.upload(g)
+        ref = oracle.cc(g)
+        for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
+            lab, rep = dg.cc(variant="union_find", loop=loop)
+            np.testing.assert_array_equal(lab, ref, err_msg=f"{name} {loop}")
+            assert rep.iterations == 2  # hook launch, compress launch
+            lab, rep = dg.cc(variant="heuristic", loop=loop)
+            np.testing.assert_array_equal(lab, ref, err_msg=f"{name} heuristic {loop}")
+        with pytest.raises(i2.I2Error) as e:
+            dg.bfs(0, variant="union_find")
+        assert e.value.status == i2._capi.I2_ERR_UNSUPPORTED
+        dg.free()
+
+
+@pytest.mark.parametrize("name", ["grid", "rmat14"])
+def test_switching_style_at_any_iteration(gpu, seeded, name):
+    # The frontier contract lets a selector change style at any iteration. Run
+    # style a for the first k iterations and style b after (then_at,
+    # then_variant), for several pairs and switch points: results must not
+    # change. For CC this includes union-find from a label-propagation state.
+    g = seeded[name]
+    dg = i2.DeviceGraph.upload(g)
+    src = int(np.argmax(g.degrees()))
+    ref = {"bfs": oracle.bfs(g, src), "sssp": oracle.sssp(g, src), "cc": oracle.cc(g)}
+    pairs = [(2, 4), (4, 2), (0, 6), (6, 3), (7, 1), (5, 2), (2, 8), (4, 8), (6, 8)]
+    for a, b in pairs:
+        for k in (1, 2, 3, 5):
+            for an in ("bfs", "sssp", "cc"):
+                if not (_for(an, a) and _for(an, b)):
+                    continue
+                src_arg = () if an == "cc" else (src,)
+                out, _ = getattr(dg, an)(*src_arg, variant=a, then_variant=b, then_at=k)
+                np.testing.assert_array_equal(out, ref[an], err_msg=f"{name} {an} {a}->{b} at {k}")
     dg.free()
