@@ -52,7 +52,7 @@ typedef struct {
 } i2_eclgraph;
 
 /* Algorithms. */
-enum { I2_BFS = 0, I2_SSSP = 1, I2_CC = 2 };
+enum { I2_BFS = 0, I2_SSSP = 1, I2_CC = 2, I2_MIS = 3 };
 
 /* Relaxation variants (styles). Every variant reaches the same fixed point. */
 enum {
@@ -195,8 +195,15 @@ int i2_graph_free(i2_graph* g);
 int i2_bfs(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep);
 int i2_sssp(i2_graph* g, int src, int* dist, const i2_opts* opts, i2_report* rep);
 int i2_cc(i2_graph* g, int* label, const i2_opts* opts, i2_report* rep);
+/* Maximal independent set (replaces GPUmis_vertex, include/mis_vertex_cuda.h:52,
+   and GPUmis_edge, include/mis_edge_cuda.h:54): status[v] = 1 in the set, 2 not,
+   the set the reference's deterministic CUDA MIS variants converge to (priority
+   hash(v + 712313887) as int, ties to the larger ID). Symmetric graphs only
+   (I2_ERR_UNSUPPORTED otherwise); opts->variant is ignored (one style: a warp
+   per frontier vertex). */
+int i2_mis(i2_graph* g, int* status, const i2_opts* opts, i2_report* rep);
 /* Same, with the result left in (or copied to) DEVICE memory; out_dev may be NULL
-   to keep the result only inside the engine. src is ignored for I2_CC. */
+   to keep the result only inside the engine. src is ignored for I2_CC and I2_MIS. */
 int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* opts, i2_report* rep);
 /* Records of the last traversal run with record_iters = 1. */
 int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n);

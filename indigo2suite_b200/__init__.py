@@ -25,6 +25,7 @@ import numpy as np
 
 from . import _capi as capi
 from ._capi import (I2_AUTO_HEURISTIC, I2_AUTO_LEARNED, I2_BFS, I2_CC, I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH,
+                    I2_MIS, MIS_IN, MIS_OUT,
                     I2_NUM_VARIANTS, I2_SSSP, VARIANTS)
 
 lib = capi.load()
@@ -33,7 +34,8 @@ __all__ = [
     "I2Error", "ECLGraph", "DeviceGraph", "Batch", "read_eclgraph", "write_eclgraph", "gen_er", "gen_rmat",
     "gen_grid", "gen_rmat_n", "synth_weights", "build_sp", "VARIANTS", "variant_id", "GPUbfs_vertex", "GPUbfs_edge",
     "GPUsssp_vertex", "GPUsssp_edge", "GPUcc_vertex", "GPUcc_edge", "mlp_param_count", "mlp_loss_grad",
-    "mlp_train", "mlp_predict", "mlp_set_params", "device_count", "I2_BFS", "I2_SSSP", "I2_CC",
+    "mlp_train", "mlp_predict", "mlp_set_params", "device_count", "I2_BFS", "I2_SSSP", "I2_CC", "I2_MIS",
+    "MIS_IN", "MIS_OUT", "GPUmis_vertex", "GPUmis_edge", "mis_priority",
     "I2_AUTO_HEURISTIC", "I2_AUTO_LEARNED", "I2_NUM_VARIANTS", "I2_LOOP_GRAPH", "I2_LOOP_HOST", "I2_LOOP_RELAUNCH",
 ]
 
@@ -270,10 +272,12 @@ class DeviceGraph:
             st = lib.i2_bfs(self._h, src, _iptr(dist), C.byref(o), C.byref(r))
         elif algo == I2_SSSP:
             st = lib.i2_sssp(self._h, src, _iptr(dist), C.byref(o), C.byref(r))
-        else:
+        elif algo == I2_CC:
             st = lib.i2_cc(self._h, _iptr(dist), C.byref(o), C.byref(r))
+        else:
+            st = lib.i2_mis(self._h, _iptr(dist), C.byref(o), C.byref(r))
         if st not in (capi.I2_OK,):
-            raise I2Error(st, ["bfs", "sssp", "cc"][algo])
+            raise I2Error(st, ["bfs", "sssp", "cc", "mis"][algo])
         return dist, _report(r, st)
 
     def bfs(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
@@ -287,6 +291,10 @@ class DeviceGraph:
     def cc(self, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
            then_variant=None, then_at: int = 0):
         return self._run(I2_CC, 0, variant, loop, iter_cap, record, stream, out, 0, then_variant, then_at)
+
+    def mis(self, loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None):
+        """Maximal independent set: status per vertex, MIS_IN (1) or MIS_OUT (2)."""
+        return self._run(I2_MIS, 0, "vp_warp", loop, iter_cap, record, stream, out)
 
     def run_device(self, algo: int, src: int = 0, out_ptr: int = 0, variant="vp_cta", loop=I2_LOOP_GRAPH,
                    iter_cap=0, record=False, stream=None, report: bool = True, delta: int = 0) -> Report | None:
@@ -415,6 +423,29 @@ def GPUcc_vertex(g: DeviceGraph, label: np.ndarray, variant=None) -> float:
 
 def GPUcc_edge(g: DeviceGraph, label: np.ndarray, sp: np.ndarray | None = None, variant=None) -> float:
     return _mirror(I2_CC, 0, g, label, "edge_topo" if variant is None else variant)
+
+
+def mis_priority(v: np.ndarray) -> np.ndarray:
+    """Priorities the reference's CUDA MIS codes give vertices (int32)."""
+    x = (np.asarray(v, np.uint64) + 712313887) & 0xFFFFFFFF
+    for _ in range(2):
+        x = (((x >> 16) ^ x) * 0x45D9F3B) & 0xFFFFFFFF
+    x = (x >> 16) ^ x
+    return x.astype(np.uint32).view(np.int32)
+
+
+def GPUmis_vertex(g: DeviceGraph, priority: np.ndarray, status: np.ndarray) -> float:
+    """Mirror of the reference's GPUmis_vertex(g, priority, status): fills both
+    host arrays (priority as the reference computes it) and returns seconds."""
+    priority[: g.nodes] = mis_priority(np.arange(g.nodes))
+    _, rep = g._run(I2_MIS, 0, "vp_warp", I2_LOOP_GRAPH, 0, False, None, status)
+    return rep.seconds
+
+
+def GPUmis_edge(g: DeviceGraph, sp, priority: np.ndarray, status: np.ndarray) -> float:
+    """Mirror of GPUmis_edge(g, sp, priority, status); sp is accepted for
+    signature parity (the engine needs none for MIS)."""
+    return GPUmis_vertex(g, priority, status)
 
 
 # ---------------------------------------------------------------------------

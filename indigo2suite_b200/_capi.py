@@ -26,7 +26,8 @@ I2_ERR_OVERFLOW = 9
 I2_ERR_CAPACITY = 10
 I2_ERR_STALL = 11
 
-I2_BFS, I2_SSSP, I2_CC = 0, 1, 2
+I2_BFS, I2_SSSP, I2_CC, I2_MIS = 0, 1, 2, 3
+MIS_IN, MIS_OUT = 1, 2  # status values of i2_mis (the reference's included / excluded)
 
 I2_AUTO_HEURISTIC = -1
 I2_AUTO_LEARNED = -2
@@ -103,6 +104,7 @@ SIGNATURES = {
     "i2_bfs": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_sssp": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_cc": (_I, [_P, _PI, C.POINTER(Opts), C.POINTER(Report)]),
+    "i2_mis": (_I, [_P, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_run_device": (_I, [_P, _I, _I, C.c_void_p, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_get_records": (_I, [_P, C.POINTER(IterRecord), _I, _PI]),
     "i2_sweep": (_I, [_P, _I, _I, _I, _I, C.POINTER(IterRecord), _PF, _I, _PI]),

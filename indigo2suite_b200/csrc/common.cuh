@@ -43,7 +43,29 @@ constexpr int kMaxVariants = 16;
 constexpr int kFeatures = 16;        // selector input width
 constexpr int kHidden = 64;          // selector hidden width (two layers)
 
-enum Algo { kBFS = 0, kSSSP = 1, kCC = 2 };
+enum Algo { kBFS = 0, kSSSP = 1, kCC = 2, kMIS = 3 };
+
+// Maximal independent set: status per vertex, the reference's undecided /
+// included / excluded (include/mis_vertex_cuda.h:52-54), and the priority its
+// CUDA codes give vertex v (hash(v + 712313887) read as int, e.g.
+// MIS_CUDA_V_Data_Pull_Determ_..._Thread.cu:51; the hash is a published
+// integer mixing function: two rounds of xor-shift by 16 and multiply by
+// 0x45d9f3b, then a final xor-shift). Neighbour u outranks v when its
+// priority is larger, or equal with a larger ID (:70).
+constexpr int kMisUndecided = 0;
+constexpr int kMisIn = 1;
+constexpr int kMisOut = 2;
+
+__device__ __forceinline__ int mis_priority(int v) {
+  unsigned x = (unsigned)v + 712313887u;
+  x = ((x >> 16) ^ x) * 0x45d9f3bu;
+  x = ((x >> 16) ^ x) * 0x45d9f3bu;
+  return (int)((x >> 16) ^ x);
+}
+
+__device__ __forceinline__ bool mis_outranks(int u, int pu, int v, int pv) {
+  return pu > pv || (pu == pv && u > v);
+}
 
 enum Variant {
   kVPThread = 0,     // vertex push, data-driven, thread per frontier vertex

@@ -50,9 +50,11 @@ __global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
   for (long long base = (long long)blockIdx.x * kBlock; base < V; base += (long long)gridDim.x * kBlock) {
     const int v = (int)base + threadIdx.x;
     const bool in = v < V;
-    if (in) c.dist[v] = (ALG == kCC) ? v : kInf;
-    if (ALG == kCC) {
-      const int deg = in ? c.g.nindex[v + 1] - c.g.nindex[v] : 0;
+    constexpr bool kAll = ALG == kCC || ALG == kMIS;  // every vertex starts in F_0
+    const int deg = (kAll && in) ? c.g.nindex[v + 1] - c.g.nindex[v] : 0;
+    // MIS: a vertex without neighbours is in the set at once
+    if (in) c.dist[v] = ALG == kCC ? v : ALG == kMIS ? (deg == 0 ? kMisIn : kMisUndecided) : kInf;
+    if (kAll) {
       const bool put = in && deg > 0;  // vertices without edges are already final
       const unsigned word = __ballot_sync(0xffffffffu, put);
       if ((threadIdx.x & 31) == 0 && word) c.bm[0][v >> 5] = word;
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
       stage_flush(c, s, 0);
     }
   }
-  if (ALG == kCC) {
+  if (ALG == kCC || ALG == kMIS) {
     stage_flush(c, s, 0);
     acc_reduce(a, s);
     if (threadIdx.x == 0) {
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(kBlock) k_fill(Ctx c) {
 template <int ALG>
 __global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
   Ctl* ctl = c.ctl;
-  if (ALG != kCC) {
+  if (ALG != kCC && ALG != kMIS) {
     const int ns = c.srcs ? ctl->nsrc : 1;
     for (int j = threadIdx.x; j < ns; j += blockDim.x) {
       const int v = c.srcs ? c.srcs[j] : ctl->src;
@@ -299,25 +301,28 @@ static KernelFn relax_fn(int v) {
 static KernelFn dispatch_kernel(int algo) {
   if (algo == kBFS) return relax_dispatch<kBFS>;
   if (algo == kSSSP) return relax_dispatch<kSSSP>;
-  return relax_dispatch<kCC>;
+  return relax_dispatch<kCC>;  // MIS has one style and never dispatches
 }
 
 KernelFn relax_kernel(int algo, int v, bool near_far) {
   if (near_far && algo == kSSSP && v == kVPCta) return relax_near_far;
   if (algo == kBFS) return relax_fn<kBFS>(v);
   if (algo == kSSSP) return relax_fn<kSSSP>(v);
-  return relax_fn<kCC>(v);
+  if (algo == kCC) return relax_fn<kCC>(v);
+  return relax_mis;  // one style
 }
 
 static KernelFn fill_kernel(int algo) {
   if (algo == kBFS) return k_fill<kBFS>;
   if (algo == kSSSP) return k_fill<kSSSP>;
-  return k_fill<kCC>;
+  if (algo == kCC) return k_fill<kCC>;
+  return k_fill<kMIS>;
 }
 static KernelFn seed_kernel(int algo) {
   if (algo == kBFS) return k_seed<kBFS>;
   if (algo == kSSSP) return k_seed<kSSSP>;
-  return k_seed<kCC>;
+  if (algo == kCC) return k_seed<kCC>;
+  return k_seed<kMIS>;
 }
 
 // ---------------------------------------------------------------------------
@@ -851,18 +856,27 @@ static int fill_report(i2_graph* g, cudaStream_t s, int algo, i2_report* rep, do
 int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
                   i2_report* rep) {
   if (!g) return I2_ERR_ARG;
-  if (algo < I2_BFS || algo > I2_CC) return I2_ERR_ARG;
+  if (algo < I2_BFS || algo > I2_MIS) return I2_ERR_ARG;
   I2_CK(cudaSetDevice(g->device));
   i2_opts o{};
   if (opts) o = *opts;
   if (o.loop_mode < I2_LOOP_GRAPH || o.loop_mode > I2_LOOP_RELAUNCH) return I2_ERR_ARG;
-  if (algo != I2_CC && !srcs_host && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
+  const bool sourced = algo == I2_BFS || algo == I2_SSSP;
+  if (sourced && !srcs_host && (src < 0 || src >= g->g.nodes)) return I2_ERR_ARG;
   if (algo == I2_SSSP) {
     if (!g->g.eweight) return I2_ERR_ARG;
     if (g->gs.wmin < 0) return I2_ERR_UNSUPPORTED;
   }
   int st = ensure_workspace(g);
   if (st) return st;
+  if (algo == I2_MIS) {  // one style; the set is defined on undirected graphs
+    st = ensure_symmetry(g);
+    if (st) return st;
+    if (g->gs.symmetric != 1) return I2_ERR_UNSUPPORTED;
+    o.variant = kVPWarp;
+    o.then_at = 0;
+    o.sssp_delta = 0;
+  }
   int mode = 0, variant = o.variant;
   if (variant == I2_AUTO_HEURISTIC) mode = 1;
   else if (variant == I2_AUTO_LEARNED) mode = 2;
@@ -1332,8 +1346,12 @@ int i2_cc(i2_graph* g, int* label, const i2_opts* opts, i2_report* rep) {
   return run_host_out(g, I2_CC, 0, label, opts, rep);
 }
 
+int i2_mis(i2_graph* g, int* status, const i2_opts* opts, i2_report* rep) {
+  return run_host_out(g, I2_MIS, 0, status, opts, rep);
+}
+
 int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* opts, i2_report* rep) {
-  int st = run_traversal(g, algo, algo == I2_CC ? 0 : src, nullptr, 0, opts, rep);
+  int st = run_traversal(g, algo, (algo == I2_CC || algo == I2_MIS) ? 0 : src, nullptr, 0, opts, rep);
   if (st && st != I2_ERR_ITER_CAP) return st;
   if (out_dev) {
     cudaStream_t s = (opts && opts->stream) ? (cudaStream_t)opts->stream : g->stream;

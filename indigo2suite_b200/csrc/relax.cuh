@@ -1124,6 +1124,78 @@ __device__ __forceinline__ bool body_union(const Ctx& c, Stage& s) {
 }
 
 // ---------------------------------------------------------------------------
+// Maximal independent set (kMIS; one style). A warp per frontier vertex v
+// still undecided: its lanes scan v's neighbours for ones that outrank v. If one
+// of them is in the set, v is out; if none is undecided (all out, or there are
+// none), v is in; otherwise v waits. A vertex that decides pushes its undecided
+// neighbours into the next frontier, so a waiting vertex is examined again as
+// soon as a neighbour that outranks it decides. Decisions depend only on
+// outranking vertices, whose decisions are final, so the set is the greedy one
+// in decreasing rank whatever the order of the updates.
+__device__ __forceinline__ bool body_mis(const Ctx& c, EBShared& sh) {
+  EpiStage& s = sh.s;
+  block_prologue(c);
+  const int i = c.ctl->iter;
+  const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
+  const int n = slot_size(c.ctl->slot[cur].packed);
+  const int active = active_blocks(c, old, ((long long)n + kWarpsPerBlock - 1) / kWarpsPerBlock);
+  if (blockIdx.x >= active) return idle_epilogue(c, s, i, cur, nxt, old);
+  if (threadIdx.x == 0) s.last = 0;
+  Acc a;
+  acc_init(a);
+  clear_old(c, old, active);
+  const int lane = threadIdx.x & 31;
+  WarpStage& ws = sh.wss[threadIdx.x >> 5];
+  if (lane == 0) ws.n = 0;
+  __syncwarp();
+  const int* wl = c.wl[cur];
+  volatile int* st = c.dist;
+  const int* __restrict__ nl = c.g.nlist;
+  const long long stride = (long long)active * kWarpsPerBlock;
+  for (long long k = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); k < n; k += stride) {
+    const int v = wl[k];
+    if (st[v] != kMisUndecided) continue;  // warp-uniform
+    const int pv = mis_priority(v);
+    const int b = c.g.nindex[v], e = c.g.nindex[v + 1];
+    bool in_set = false, waiting = false;
+    for (int base = b; base < e; base += kWarp) {
+      const int j = base + lane;
+      if (j < e) {
+        const int u = ld_adj(nl + j);
+        if (u != v && mis_outranks(u, mis_priority(u), v, pv)) {
+          const int su = st[u];
+          in_set |= su == kMisIn;
+          waiting |= su == kMisUndecided;
+        }
+      }
+      if (__any_sync(0xffffffffu, in_set)) break;  // v is out whatever the rest holds
+    }
+    const bool out = __any_sync(0xffffffffu, in_set);
+    const bool wait = !out && __any_sync(0xffffffffu, waiting);
+    if (wait) continue;
+    if (lane == 0) st[v] = out ? kMisOut : kMisIn;
+    a.visited += lane == 0;
+    for (int base = b; base < e; base += kWarp) {
+      const int j = base + lane;
+      if (j < e) {
+        const int u = ld_adj(nl + j);
+        if (u != v && st[u] == kMisUndecided) {
+          const unsigned bit = 1u << (u & 31);
+          unsigned* w = &c.bm[nxt][u >> 5];
+          if (!(*(volatile unsigned*)w & bit) && !(atomicOr(w, bit) & bit))
+            warp_stage_entry(c, ws, a, nxt, u, c.g.nindex[u + 1] - c.g.nindex[u]);
+        }
+      }
+      __syncwarp();
+      if (ws.n >= kWarpQueue / 2) warp_flush(c, ws, nxt);
+    }
+  }
+  warp_flush(c, ws, nxt);
+  __syncthreads();
+  return block_epilogue(c, s, a, i, cur, nxt, old, active);
+}
+
+// ---------------------------------------------------------------------------
 // Kernel wrappers.
 template <int ALG, int VAR>
 __global__ void __launch_bounds__(kBlock) relax_push(Ctx c) {
@@ -1135,6 +1207,11 @@ template <int ALG>
 __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_edge_balanced(Ctx c) {
   __shared__ EBShared sh;
   body_edge_balanced<ALG>(c, sh);
+}
+
+static __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_mis(Ctx c) {
+  __shared__ EBShared sh;
+  body_mis(c, sh);
 }
 
 // Edge-balanced SSSP push with near/far ordering (Ctl::delta > 0).
@@ -1203,19 +1280,23 @@ __device__ __forceinline__ void grid_wait(Ctl* ctl, unsigned gen) {
 
 template <int ALG, int VAR, bool DEFER>
 __device__ __forceinline__ bool run_body(const Ctx& c, AnyShared& sh) {
-  const int v = VAR >= 0 ? VAR : *(volatile int*)&c.ctl->variant;  // uniform: written before the release
-  switch (v) {
-    case kVPThread: return body_push<ALG, kVPThread>(c, sh.st);
-    case kVPWarp: return body_push<ALG, kVPWarp>(c, sh.st);
-    case kVPCta: return body_edge_balanced<ALG, DEFER>(c, sh.eb);
-    case kVPBlock: return body_push<ALG, kVPBlock>(c, sh.st);
-    case kPullFrontier: return body_pull<ALG, true>(c, sh.st);
-    case kPullTopo: return body_pull<ALG, false>(c, sh.st);
-    case kEdgeTopo: return body_edge_topo<ALG>(c, sh.st);
-    case kUnionFind:
-      if constexpr (ALG == kCC) return body_union<ALG>(c, sh.st);
-      [[fallthrough]];  // not allowed for BFS/SSSP
-    default: return body_push_topo<ALG>(c, sh.st);
+  if constexpr (ALG == kMIS) {
+    return body_mis(c, sh.eb);  // one style
+  } else {
+    const int v = VAR >= 0 ? VAR : *(volatile int*)&c.ctl->variant;  // uniform: written before the release
+    switch (v) {
+      case kVPThread: return body_push<ALG, kVPThread>(c, sh.st);
+      case kVPWarp: return body_push<ALG, kVPWarp>(c, sh.st);
+      case kVPCta: return body_edge_balanced<ALG, DEFER>(c, sh.eb);
+      case kVPBlock: return body_push<ALG, kVPBlock>(c, sh.st);
+      case kPullFrontier: return body_pull<ALG, true>(c, sh.st);
+      case kPullTopo: return body_pull<ALG, false>(c, sh.st);
+      case kEdgeTopo: return body_edge_topo<ALG>(c, sh.st);
+      case kUnionFind:
+        if constexpr (ALG == kCC) return body_union<ALG>(c, sh.st);
+        [[fallthrough]];  // not allowed for BFS/SSSP
+      default: return body_push_topo<ALG>(c, sh.st);
+    }
   }
 }
 

@@ -30,6 +30,7 @@ static KernelFn resident_fn(int v) {
 // Kernel of a resident traversal: fixed style v (mode 0) or the per-iteration
 // pick (v < 0).
 KernelFn resident_kernel(int algo, int v, bool near_far) {
+  if (algo == kMIS) return relax_resident<kMIS, kVPWarp>;  // one style
   if (near_far && algo == kSSSP && v == kVPCta) return relax_resident<kSSSP, kVPCta, true>;
   if (algo == kBFS) return resident_fn<kBFS>(v);
   if (algo == kSSSP) return resident_fn<kSSSP>(v);

@@ -10,7 +10,7 @@
 // without copying them and returns the engine's device time in seconds. Only
 // the SSSP harnesses upload the weights (include/sssp_vertex_cuda.h:122-125);
 // in the BFS and CC harnesses d_g.eweight is still the host array from the file
-// reader, so those shims pass no weights.
+// reader, so those shims pass no weights (MIS needs none).
 //
 // $I2_VARIANT selects the style: a variant name (vp_thread, vp_warp, vp_cta,
 // vp_block, pull_frontier, pull_topo, edge_topo, push_topo), "heuristic"
@@ -36,7 +36,7 @@ static void i2shim_fail(const char* what, int st) {
   std::exit(-1);
 }
 
-// algo: I2_BFS / I2_SSSP / I2_CC. The CSR arrays in g are device pointers.
+// algo: I2_BFS / I2_SSSP / I2_CC / I2_MIS. The CSR arrays in g are device pointers.
 static double i2shim_run(int algo, int src, int nodes, int edges, int* nindex, int* nlist, int* eweight, int* out,
                          int fallback_variant) {
   i2_eclgraph d = {nodes, edges, nindex, nlist, eweight};
@@ -50,7 +50,8 @@ static double i2shim_run(int algo, int src, int nodes, int edges, int* nindex, i
   std::memset(&r, 0, sizeof(r));
   if (algo == I2_BFS) st = i2_bfs(h, src, out, &o, &r);
   else if (algo == I2_SSSP) st = i2_sssp(h, src, out, &o, &r);
-  else st = i2_cc(h, out, &o, &r);
+  else if (algo == I2_CC) st = i2_cc(h, out, &o, &r);
+  else st = i2_mis(h, out, &o, &r);
   i2_graph_free(h);
   if (st != I2_OK) i2shim_fail("run", st);
   std::printf("iterations: %d\n", r.iterations);

@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         _lib.oracle_cc_check.argtypes = [C.c_int, P, P, P]
         _lib.oracle_synth_weights.argtypes = [C.c_int, P, P, P]
         _lib.oracle_sp.argtypes = [C.c_int, P, P]
+        _lib.oracle_mis.argtypes = [C.c_int, P, P, C.c_int, P]
+        _lib.oracle_mis_priority.argtypes = [C.c_int]
         _lib.oracle_synth_weights.restype = None
         _lib.oracle_sp.restype = None
     return _lib
@@ -82,6 +84,49 @@ def cc(g) -> np.ndarray:
     rc = lib().oracle_cc_minlabel(g.nodes, _p(ni), _p(nl), _p(out))
     assert rc == 0, rc
     return out
+
+
+def mis(g, unsigned_priority: bool = False) -> np.ndarray:
+    """Status per vertex: 1 in the maximal independent set, 2 excluded. The
+    reference's CUDA MIS codes compare priorities as int (the default here),
+    its CPU codes as unsigned int."""
+    ni, nl = _csr(g)
+    out = np.empty(g.nodes, np.int32)
+    rc = lib().oracle_mis(g.nodes, _p(ni), _p(nl), int(unsigned_priority), _p(out))
+    assert rc == 0, rc
+    return out
+
+
+def ref_cuda_mis(g) -> np.ndarray:
+    """The status array of the reference's CUDA MIS variant
+    (MIS_CUDA_V_Data_Pull_Determ_..._Thread.cu via _ref/libref_cuda_mis.so);
+    needs a GPU."""
+    L = C.CDLL(str(REF_OUT / "libref_cuda_mis.so"))
+    P = C.POINTER(C.c_int)
+    L.ref_cuda_mis.argtypes = [C.c_int, C.c_int, P, P, P]
+    L.ref_cuda_mis.restype = C.c_double
+    ni, nl = _csr(g)
+    out = np.empty(g.nodes, np.int32)
+    import sys
+
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference driver prints its iteration count
+    try:
+        t = L.ref_cuda_mis(g.nodes, g.edges, _p(ni), _p(nl), _p(out))
+        C.CDLL(None).fflush(None)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    if t < 0:
+        raise RuntimeError("reference CUDA MIS could not allocate")
+    return out
+
+
+def mis_priority(v: int) -> int:
+    return int(lib().oracle_mis_priority(int(v)))
 
 
 def cc_check(g, label: np.ndarray) -> int:
@@ -232,7 +277,7 @@ _cpu = {}
 
 def ref_cpu_run(name: str, g, src: int, threads: int, sp: np.ndarray | None = None) -> tuple[float, np.ndarray]:
     """Run the reference CPU program `name` (sssp_edge_cpp, sssp_vertex_cpp,
-    sssp_edge_omp, bfs_cpp, bfs_omp, cc_cpp, cc_omp) once; returns its own
+    sssp_edge_omp, bfs_cpp, bfs_omp, cc_cpp, cc_omp, mis_cpp) once; returns its own
     measured runtime in seconds and the result."""
     if name not in _cpu:
         L = C.CDLL(str(REF_OUT / f"libref_cpu_{name}.so"))

@@ -15,6 +15,17 @@
  *   oracle_cc_minlabel  the minimum-ID labelling that every reference CC variant
  *                       converges to (label[v] = v, then atomicMin(label[dst], label[src]),
  *                       e.g. CC_CUDA_E_Data_Push_..._NonDup.cu:53,71)
+ *   oracle_mis          the maximal independent set every deterministic reference MIS
+ *                       variant converges to: priority(v) = hash(v + 712313887) read as
+ *                       int (include/mis_vertex_cuda.h:170-176, e.g.
+ *                       MIS_CUDA_V_Data_Pull_Determ_..._Thread.cu:51), neighbour u ranks
+ *                       above v when its priority is larger or equal with a larger ID
+ *                       (:70); v is in the set iff no higher-ranked neighbour is: the
+ *                       greedy set in decreasing rank, computed here in that order.
+ *                       Status 1 = in the set, 2 = excluded (:52-54). The CUDA variants
+ *                       compare priorities as int (their data_type); the reference's C++
+ *                       and OpenMP MIS variants as unsigned int (codes/cpp/mis-cpp/*.cpp:38),
+ *                       which gives another set: `unsigned_priority` selects that order.
  *   oracle_synth_weights include/sssp_vertex_cuda.h:127-137
  *   oracle_sp           include/bfs_edge_cuda.h:140-146
  * Distances use int32 arithmetic with two's-complement wrap, like the reference's
@@ -202,4 +213,54 @@ void oracle_synth_weights(int nodes, const int* nindex, const int* nlist, int* w
 void oracle_sp(int nodes, const int* nindex, int* sp) {
   for (int i = 0; i < nodes; i++)
     for (int j = nindex[i]; j < nindex[i + 1]; j++) sp[j] = i;
+}
+
+/* ---- maximal independent set ------------------------------------------- */
+
+/* The integer hash of the reference MIS codes (a published mixing function:
+   two rounds of xor-shift by 16 and multiply by 0x45d9f3b, then a final
+   xor-shift), applied to v + 712313887. */
+static unsigned mis_hash(unsigned x) {
+  x = ((x >> 16) ^ x) * 0x45d9f3bu;
+  x = ((x >> 16) ^ x) * 0x45d9f3bu;
+  return (x >> 16) ^ x;
+}
+
+int oracle_mis_priority(int v) { return (int)mis_hash((unsigned)v + 712313887u); }
+
+static const int* g_mis_prio;
+static int g_mis_unsigned;
+
+/* descending rank: larger priority first, then larger ID */
+static int mis_rank_cmp(const void* a, const void* b) {
+  const int u = *(const int*)a, v = *(const int*)b;
+  const int pu = g_mis_prio[u], pv = g_mis_prio[v];
+  if (pu != pv) {
+    if (g_mis_unsigned) return (unsigned)pu > (unsigned)pv ? -1 : 1;
+    return pu > pv ? -1 : 1;
+  }
+  return u > v ? -1 : (u < v ? 1 : 0);
+}
+
+int oracle_mis(int nodes, const int* nindex, const int* nlist, int unsigned_priority, int* status) {
+  if (nodes < 0) return 1;
+  int* prio = (int*)malloc(sizeof(int) * (size_t)(nodes > 0 ? nodes : 1));
+  int* order = (int*)malloc(sizeof(int) * (size_t)(nodes > 0 ? nodes : 1));
+  if (!prio || !order) { free(prio); free(order); return 2; }
+  for (int v = 0; v < nodes; ++v) { prio[v] = oracle_mis_priority(v); order[v] = v; status[v] = 0; }
+  g_mis_prio = prio;
+  g_mis_unsigned = unsigned_priority;
+  qsort(order, (size_t)nodes, sizeof(int), mis_rank_cmp);
+  for (int k = 0; k < nodes; ++k) {
+    const int v = order[k];
+    int in = 1;
+    for (int i = nindex[v]; i < nindex[v + 1]; ++i) {
+      const int u = nlist[i];
+      if (u != v && status[u] == 1) { in = 0; break; }  /* only higher-ranked vertices are decided */
+    }
+    status[v] = in ? 1 : 2;
+  }
+  free(prio);
+  free(order);
+  return 0;
 }

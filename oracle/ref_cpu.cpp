@@ -34,5 +34,14 @@ extern "C" double ref_cpu_run(int nodes, int edges, int* nindex, int* nlist, int
 #elif defined(REF_OMP_CC_VERTEX)
   omp_set_num_threads(threads);
   return CPUcc_vertex(g, dist);
+#elif defined(REF_CPP_MIS_VERTEX)
+  // the MIS driver fills a byte status per vertex (1 in the set, 2 excluded)
+  data_type* priority = new data_type[nodes > 0 ? nodes : 1];
+  unsigned char* st = new unsigned char[nodes > 0 ? nodes : 1];
+  const double t = CPPmis_vertex(g, priority, st, threads);
+  for (int v = 0; v < nodes; ++v) dist[v] = st[v];
+  delete[] priority;
+  delete[] st;
+  return t;
 #endif
 }

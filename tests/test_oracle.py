@@ -97,3 +97,48 @@ def test_minlabel_is_reachability_minimum_on_directed_graph():
     # 0 -> 1 -> 2, 3 -> 2: label = min vertex that reaches v
     g = i2.ECLGraph(4, 3, np.array([0, 1, 2, 2, 3], np.int32), np.array([1, 2, 2], np.int32))
     np.testing.assert_array_equal(oracle.cc(g), [0, 0, 0, 3])
+
+
+def _greedy_mis(g, unsigned_priority):
+    """Pure-Python restatement: vertices in decreasing rank, each in the set
+    iff no neighbour already in it."""
+    prio = i2.mis_priority(np.arange(g.nodes))
+    key = prio.view(np.uint32).astype(np.int64) if unsigned_priority else prio.astype(np.int64)
+    order = sorted(range(g.nodes), key=lambda v: (-int(key[v]), -v))
+    st = np.zeros(g.nodes, np.int32)
+    for v in order:
+        nb = g.nlist[g.nindex[v]:g.nindex[v + 1]]
+        st[v] = 2 if any(st[u] == 1 for u in nb if u != v) else 1
+    return st
+
+
+def test_mis_priority_matches_oracle():
+    vs = np.array([0, 1, 2, 77, 1 << 20, (1 << 31) - 712313888, 2_000_000_000], np.int64)
+    got = i2.mis_priority(vs)
+    assert [oracle.mis_priority(int(v)) for v in vs] == got.tolist()
+
+
+@pytest.mark.parametrize("unsigned", [False, True])
+def test_mis_oracle_is_the_greedy_set(unsigned):
+    for g in (i2.gen_er(300, 900, 2), i2.gen_rmat(9, 8, seed=3), i2.gen_grid(12, 0.1, 0.02, 5)):
+        st = oracle.mis(g, unsigned_priority=unsigned)
+        np.testing.assert_array_equal(st, _greedy_mis(g, unsigned))
+        # independent and maximal
+        for v in range(g.nodes):
+            nb = [u for u in g.nlist[g.nindex[v]:g.nindex[v + 1]] if u != v]
+            if st[v] == 1:
+                assert all(st[u] != 1 for u in nb)
+            else:
+                assert any(st[u] == 1 for u in nb)
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference programs not built")
+def test_mis_oracle_matches_reference_cpu_program():
+    # The reference's C++ MIS codes compare priorities as unsigned int; the
+    # oracle's unsigned order must give exactly their set. (Its CUDA codes
+    # compare them as int: the GPU tests pin that order against one of them.)
+    for g in (i2.gen_rmat(14, 16, seed=5), i2.gen_er(20000, 80000, 3), i2.gen_grid(96, 0.05, 0.002, 7),
+              i2.gen_rmat(16, 16, seed=2)):
+        _, ref = oracle.ref_cpu_run("mis_cpp", g, 0, 4)
+        np.testing.assert_array_equal(oracle.mis(g, unsigned_priority=True), ref)
+    assert not np.array_equal(oracle.mis(g, unsigned_priority=False), ref)  # the two orders differ

@@ -46,12 +46,23 @@ def test_reference_harness_verifies_engine(gpu, files, shim):
     for name, (path, g) in files.items():
         src = int(np.argmax(g.degrees()))
         args = [path, 1] if shim.startswith("cc") else [path, src, 1]
-        for v in ["heuristic", "vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo",
-                  "edge_topo", "push_topo"]:
+        styles = ["heuristic", "vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo",
+                  "edge_topo", "push_topo"] + (["union_find"] if shim.startswith("cc") else [])
+        for v in styles:
             rc, out = _run(f"shim_{shim}", args, {"I2_VARIANT": v})
             assert rc == 0 and "verification passed" in out, f"{shim} {name} {v}\n{out[-2000:]}"
         rc, out = _run(f"shim_{shim}", args, {"I2_LOOP": "host"})
         assert rc == 0 and "verification passed" in out, out[-2000:]
+
+
+@pytest.mark.parametrize("shim", ["mis_vertex", "mis_edge"])
+def test_reference_mis_harness_verifies_engine(gpu, files, shim):
+    # The MIS harness's verifier (independent, maximal, nothing undecided)
+    # exits non-zero with "ERROR" on a failure and prints nothing on success.
+    for name, (path, g) in files.items():
+        for env in ({}, {"I2_LOOP": "host"}):
+            rc, out = _run(f"shim_{shim}", [path, 1], env)
+            assert rc == 0 and "ERROR" not in out, f"{shim} {name} {env}\n{out[-2000:]}"
 
 
 def _summary(out):
