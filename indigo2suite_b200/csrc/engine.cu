@@ -1039,6 +1039,15 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
           I2_CK(cudaEventSynchronize(g->ev1));
           float ms = 0.f;
           I2_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+          // The launches' own device time (their iteration records), without the
+          // launch latency that the resident traversal does not pay.
+          const int nrec = v == kUnionFind ? 2 : 1;
+          if (snap.iter + nrec <= g->rec_cap) {
+            IterRec r[2];
+            I2_CK(cudaMemcpy(r, g->recs + snap.iter, sizeof(IterRec) * nrec, cudaMemcpyDeviceToHost));
+            ms = 0.f;
+            for (int j = 0; j < nrec; ++j) ms += (float)r[j].t_ns * 1e-6f;
+          }
           if (best < 0.f || ms < best) best = ms;
         }
         best *= 1e6f;  // ns

@@ -18,12 +18,18 @@ namespace i2 {
 // carries more than 1/16 of the edges (direction-optimising BFS), otherwise the
 // edge-balanced push, which measured fastest of the push styles on every
 // family tried.
+// Union-find replaces the whole traversal, so it is a choice made once, before
+// the first iteration, by both selectors; the per-iteration picks are among the
+// propagation styles.
+static __device__ bool union_find_first(const GStats& gs, int algo, int allowed, int next_iter) {
+  return algo == kCC && next_iter == 0 && ((allowed >> kUnionFind) & 1) && gs.avgdeg < 6.f;
+}
+
 static __device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, unsigned long long edges) {
   (void)size;
   const float fe = (float)edges;
   const float E = (float)gs.edges;
   auto ok = [&](int v) { return (allowed >> v) & 1; };
-  if (algo == kCC && ok(kUnionFind) && gs.avgdeg < 6.f) return kUnionFind;
   if (algo == kBFS && ok(kPullFrontier) && fe > E * (1.f / 16.f)) return kPullFrontier;
   return ok(kVPCta) ? kVPCta : kVPThread;
 }
@@ -60,6 +66,8 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
     int v = ctl->fixed_variant;
     if (mode == 3) {
       v = next_iter >= ctl->then_at ? ctl->then_variant : ctl->fixed_variant;
+    } else if ((mode == 1 || mode == 2) && union_find_first(c.gs, ctl->algo, ctl->allowed, next_iter)) {
+      v = kUnionFind;
     } else if (mode == 1 || (mode == 2 && !c.mlp)) {
       volatile Slot* sl = &ctl->slot[nxt];
       const unsigned long long p = sl->packed;
@@ -69,8 +77,8 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
       if (infer) {
         float best = 3.0e38f;
         int bv = -1;
-        for (int k = 0; k < kOut; ++k)
-          if (((ctl->allowed >> k) & 1) && y[k] < best) {
+        for (int k = 0; k < kOut; ++k)  // per-iteration styles only (see union_find_first)
+          if (k != kUnionFind && ((ctl->allowed >> k) & 1) && y[k] < best) {
             best = y[k];
             bv = k;
           }

@@ -95,6 +95,7 @@ def record(specs, algos=("bfs", "sssp", "cc"), follows=(I2_AUTO_HEURISTIC, 2), r
         for an in algos:
             for fol in follows:
                 recs, times = dg.sweep(ALGOS[an], src, follow=fol, reps=reps, cap=1 << 14)
+                times = _union_find_equivalent(recs, times)
                 for r, t in zip(recs, times):
                     ok = t > 0
                     if not ok.any():
@@ -108,6 +109,30 @@ def record(specs, algos=("bfs", "sssp", "cc"), follows=(I2_AUTO_HEURISTIC, 2), r
         if log:
             log(f"[{gi + 1}/{len(specs)}] {spec.name}: V={g.nodes} E={g.edges} rows={rows} ({time.time() - t0:.1f}s)")
     return (np.asarray(X, np.float32), np.asarray(T, np.float32), np.asarray(M, np.float32), meta)
+
+
+UF = VARIANTS.index("union_find")
+
+
+def _union_find_equivalent(recs, times):
+    """(Union-find is chosen before the first iteration by a rule shared with
+    the heuristic, so the selector reads this column only as training data.)
+    Union-find finishes the whole traversal in one choice, so its time is
+    not comparable with one iteration of another style. Along the followed
+    trajectory (per-iteration times f_k, remaining time R_k after iteration
+    k), its time at iteration k is scaled to the share of the remaining work
+    that one iteration represents: t_uf * f_k / (f_k + R_k). The selector then
+    prefers it exactly when t_uf < f_k + R_k, i.e. when it beats finishing
+    along the trajectory."""
+    times = np.array(times, np.float64, copy=True)
+    if len(recs) == 0:
+        return times
+    f = np.array([times[k, r["variant"]] if times[k, r["variant"]] > 0 else 0.0 for k, r in enumerate(recs)])
+    rest = np.concatenate([np.cumsum(f[::-1])[::-1][1:], [0.0]])
+    for k in range(len(recs)):
+        if times[k, UF] > 0 and f[k] > 0:
+            times[k, UF] *= f[k] / (f[k] + rest[k])
+    return times
 
 
 def train(X, T, M, epochs: int = 200, batch: int = 512, lr: float = 2e-3, seed: int = 1):

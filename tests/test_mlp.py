@@ -83,3 +83,19 @@ def test_device_training_reduces_loss_and_inference_matches_oracle(gpu):
         assert abs(y[r, choice[r]] - y[r, ref[r]]) < 1e-4
     assert len(mism) <= 2
     assert not np.any(choice == 3)
+
+
+def test_union_find_time_is_scaled_to_one_iterations_share():
+    from indigo2suite_b200 import selector
+
+    uf = selector.UF
+    times = np.full((3, i2.I2_NUM_VARIANTS), -1.0)
+    times[:, 2] = [10.0, 20.0, 30.0]  # the followed style
+    times[:, uf] = [60.0, 40.0, 100.0]
+    recs = [{"variant": 2}] * 3
+    out = selector._union_find_equivalent(recs, times)
+    # remaining after k: 50, 30, 0 -> uf scaled by f/(f+rest): 10/60, 20/50, 30/30
+    np.testing.assert_allclose(out[:, uf], [10.0, 16.0, 100.0])
+    np.testing.assert_array_equal(out[:, 2], times[:, 2])
+    # union-find is preferred exactly when it beats finishing along the trajectory
+    assert out[0, uf] <= out[0, 2] and out[1, uf] < out[1, 2] and out[2, uf] > out[2, 2]
