@@ -157,7 +157,7 @@ struct Ctl {
   int uf_phase;             // union-find CC: 1 after the hook launch (the compress launch follows)
   int then_at;              // mode 3: iteration from which then_variant runs
   int then_variant;
-  int pad2;
+  int uf_giant;             // union-find CC: root of the sampled largest tree
   // Resident launches (one launch runs every iteration, the grid meeting at
   // a barrier between them).
   unsigned bar_gen;         // barrier generation, bumped once per iteration

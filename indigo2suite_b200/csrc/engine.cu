@@ -615,7 +615,7 @@ static int allowed_mask(const i2_graph* g, int algo) {
   int m = 0;
   for (int v = 0; v < kNumVariants; ++v) m |= 1 << v;
   if (g->gs.symmetric != 1) m &= ~((1 << kPullFrontier) | (1 << kPullTopo) | (1 << kUnionFind));
-  if (!g->d_sp) m &= ~((1 << kEdgeTopo) | (1 << kUnionFind));
+  if (!g->d_sp) m &= ~(1 << kEdgeTopo);
   if (algo != I2_CC) m &= ~(1 << kUnionFind);
   return m;
 }
@@ -886,7 +886,7 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     if (mode != 0 || o.then_variant < 0 || o.then_variant >= kNumVariants) return I2_ERR_ARG;
     mode = 3;
   }
-  if (mode != 0 || variant == kEdgeTopo || variant == kUnionFind) {
+  if (mode != 0 || variant == kEdgeTopo) {
     st = ensure_sp(g);
     if (st) return st;
   }
@@ -1034,16 +1034,19 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
           I2_CK(cudaMemcpyAsync(g->bm[0], g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words, cudaMemcpyDeviceToDevice, s));
           I2_CK(cudaEventRecord(g->ev0, s));
           dk<<<dgrid, kBlock, 0, s>>>(c);
-          if (v == kUnionFind) dk<<<dgrid, kBlock, 0, s>>>(c);  // its compress launch belongs to it
+          if (v == kUnionFind) {  // its later launches belong to it
+            dk<<<dgrid, kBlock, 0, s>>>(c);
+            dk<<<dgrid, kBlock, 0, s>>>(c);
+          }
           I2_CK(cudaEventRecord(g->ev1, s));
           I2_CK(cudaEventSynchronize(g->ev1));
           float ms = 0.f;
           I2_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
           // The launches' own device time (their iteration records), without the
           // launch latency that the resident traversal does not pay.
-          const int nrec = v == kUnionFind ? 2 : 1;
+          const int nrec = v == kUnionFind ? 3 : 1;
           if (snap.iter + nrec <= g->rec_cap) {
-            IterRec r[2];
+            IterRec r[3];
             I2_CK(cudaMemcpy(r, g->recs + snap.iter, sizeof(IterRec) * nrec, cudaMemcpyDeviceToHost));
             ms = 0.f;
             for (int j = 0; j < nrec; ++j) ms += (float)r[j].t_ns * 1e-6f;

@@ -11,10 +11,9 @@ namespace i2 {
 // ---------------------------------------------------------------------------
 // Selection of the next variant.
 
-// Fixed frontier-size rule: union-find for CC on symmetric graphs of mean
-// degree below 6 (grid-like, high diameter: label propagation needs hundreds
-// of iterations there, while on RMAT and ER graphs it converges in a handful
-// and union-find measured 2-4x slower), bottom-up pull for BFS levels whose frontier
+// Fixed frontier-size rule: union-find for CC on symmetric graphs (measured
+// 2.5-23x faster than the best propagation style on RMAT, ER and grid graphs
+// of 2^22 vertices and more, within 2x either way on 2^18), bottom-up pull for BFS levels whose frontier
 // carries more than 1/16 of the edges (direction-optimising BFS), otherwise the
 // edge-balanced push, which measured fastest of the push styles on every
 // family tried.
@@ -22,7 +21,8 @@ namespace i2 {
 // the first iteration, by both selectors; the per-iteration picks are among the
 // propagation styles.
 static __device__ bool union_find_first(const GStats& gs, int algo, int allowed, int next_iter) {
-  return algo == kCC && next_iter == 0 && ((allowed >> kUnionFind) & 1) && gs.avgdeg < 6.f;
+  (void)gs;
+  return algo == kCC && next_iter == 0 && ((allowed >> kUnionFind) & 1);
 }
 
 static __device__ int heuristic_pick(const GStats& gs, int algo, int allowed, int size, unsigned long long edges) {
@@ -103,6 +103,7 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
 static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old) {
   __shared__ int s_cond, s_force;
   Ctl* ctl = c.ctl;
+  if (ctl->variant == kUnionFind && ctl->uf_phase == 0) uf_sample_giant(c);  // whole block
   if (threadIdx.x == 0) {
     const unsigned long long t1 = globaltimer();
     const unsigned long long dt = t1 - ctl->tstart;
@@ -154,8 +155,8 @@ static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, i
     }
     int force = -1;
     if (ctl->variant == kUnionFind) {
-      if (ctl->uf_phase == 0) {  // hook launch done: the compress launch follows
-        ctl->uf_phase = 1;
+      if (ctl->uf_phase < 2) {  // the next union-find launch follows
+        ctl->uf_phase += 1;
         force = kUnionFind;
         cond = 1;
       } else {

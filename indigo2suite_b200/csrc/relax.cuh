@@ -1042,17 +1042,22 @@ __device__ __forceinline__ bool body_pull(const Ctx& c, Stage& s) {
 // result is the minimum-ID labelling that label propagation converges to,
 // reached from any propagation state in two launches.
 
-// Root of x. With `halve`, each step also points the visited vertex at its
+// Root of x. With HALVE, each step also points the visited vertex at its
 // grandparent (path halving): any ancestor is a valid label, and a vertex that
 // is not a root never becomes one again, so these plain writes cannot undo a
-// link. Loads are coherent (other threads link and halve concurrently).
+// link. The loads may be served from this SM's L1 and so be stale: a stale
+// parent is still an ancestor (links are never undone), and a vertex wrongly
+// seen as a root only makes the linking compare-and-swap fail and return its
+// true parent, from which the search continues (parents only decrease, so it
+// ends). Cached loads matter: almost every find ends at a component's root,
+// and reading that one entry from L2 every time serialises on it.
 template <bool HALVE>
 __device__ __forceinline__ int uf_find(int* p, int x) {
   for (;;) {
-    const int px = *(volatile int*)&p[x];
+    const int px = p[x];
     if (px == x) return x;
-    const int ppx = *(volatile int*)&p[px];
-    if (HALVE && ppx != px) *(volatile int*)&p[x] = ppx;
+    const int ppx = p[px];
+    if (HALVE && ppx != px) p[x] = ppx;
     x = ppx;
   }
 }
@@ -1072,6 +1077,56 @@ __device__ __forceinline__ void uf_union(int* p, int a, int b) {
   }
 }
 
+// Neighbours each vertex is linked with before the largest tree is sampled.
+constexpr int kAfforestLinks = 2;
+constexpr int kAfforestSamples = 1024;
+
+// Root of x with coherent loads (the sampling after the first hook launch).
+__device__ __forceinline__ int uf_find_fresh(int* p, int x) {
+  for (;;) {
+    const int px = *(volatile int*)&p[x];
+    if (px == x) return x;
+    x = px;
+  }
+}
+
+// Called by the whole last block of the first hook launch: the roots of
+// kAfforestSamples vertices spread over the graph, and the root held by a
+// majority of them (Boyer-Moore vote), taken as the largest tree. Any root
+// would keep the result correct; the vote only decides how many vertices the
+// second hook launch can skip.
+__device__ __forceinline__ void uf_sample_giant(const Ctx& c) {
+  __shared__ int roots[kAfforestSamples];
+  const int V = c.g.nodes;
+  for (int k = threadIdx.x; k < kAfforestSamples; k += blockDim.x)
+    roots[k] = V > 0 ? uf_find_fresh(c.dist, (int)((unsigned)mis_priority(k) % (unsigned)V)) : 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int cand = -1, cnt = 0;
+    for (int k = 0; k < kAfforestSamples; ++k) {
+      if (cnt == 0) {
+        cand = roots[k];
+        cnt = 1;
+      } else {
+        cnt += roots[k] == cand ? 1 : -1;
+      }
+    }
+    c.ctl->uf_giant = cand;
+  }
+  __syncthreads();
+}
+
+// Three launches (Ctl::uf_phase): (0) link every vertex with its first
+// kAfforestLinks neighbours, after which the last block samples the largest
+// tree; (1) link the remaining neighbours of every vertex whose root is not
+// that tree's (an edge from a skipped vertex to a vertex outside the tree is
+// linked from the other end, and an edge inside the tree changes nothing);
+// (2) set every label to its root. Links put the larger root below the
+// smaller one whatever the order, so the roots are the components' minimum
+// IDs, as in a single pass over all edges (sampling scheme of Sutton et al.,
+// "Optimizing parallel graph connectivity computation via subgraph sampling",
+// IPDPS 2018). On graphs with a giant component the second launch skips most
+// edges.
 template <int ALG>
 __device__ __forceinline__ bool body_union(const Ctx& c, Stage& s) {
   block_prologue(c);
@@ -1083,38 +1138,34 @@ __device__ __forceinline__ bool body_union(const Ctx& c, Stage& s) {
   const int active = gridDim.x;
   clear_old(c, old, active);
   int* p = c.dist;
+  const int V = c.g.nodes;
+  const int* __restrict__ nl = c.g.nlist;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (c.ctl->uf_phase == 0) {
-    // hook: every CSR entry (u, v) with v < u, four per thread, 128-bit loads
-    const int E = c.g.edges;
-    const long long units = ((long long)E + 3) >> 2;
-    const int* __restrict__ sp = c.g.sp;
-    const int* __restrict__ nl = c.g.nlist;
-    for (long long q = tid; q < units; q += stride) {
-      const long long k0 = q << 2;
-      int su[4], nv[4];
-      if (c.g.vec_ok && k0 + 3 < E) {
-        const int4 x = ld_adj(reinterpret_cast<const int4*>(sp + k0));
-        const int4 y = ld_adj(reinterpret_cast<const int4*>(nl + k0));
-        su[0] = x.x; su[1] = x.y; su[2] = x.z; su[3] = x.w;
-        nv[0] = y.x; nv[1] = y.y; nv[2] = y.z; nv[3] = y.w;
-      } else {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const long long k = k0 + r;
-          su[r] = k < E ? sp[k] : 0;
-          nv[r] = k < E ? nl[k] : 0;
-        }
+  const int phase = c.ctl->uf_phase;
+  if (phase == 0) {
+    for (long long v = tid; v < V; v += stride) {
+      const int b = c.g.nindex[v];
+      const int e = min(c.g.nindex[v + 1], b + kAfforestLinks);
+      for (int j = b; j < e; ++j) {
+        const int u = ld_adj(nl + j);
+        if (u != (int)v) uf_union(p, (int)v, u);
       }
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (nv[r] < su[r]) uf_union(p, su[r], nv[r]);
+    }
+  } else if (phase == 1) {
+    const int giant = c.ctl->uf_giant;
+    for (long long v = tid; v < V; v += stride) {
+      const int b = c.g.nindex[v] + kAfforestLinks;
+      const int e = c.g.nindex[v + 1];
+      if (b >= e || uf_find<true>(p, (int)v) == giant) continue;
+      for (int j = b; j < e; ++j) {
+        const int u = ld_adj(nl + j);
+        if (u != (int)v) uf_union(p, (int)v, u);
+      }
     }
   } else {
     // compress: read-only finds (a halving write could replace a finished
     // label with an intermediate ancestor), each thread writing its own labels
-    const int V = c.g.nodes;
     for (long long v = tid; v < V; v += stride) {
       const int r = uf_find<false>(p, (int)v);
       if (r != (int)v) p[v] = r;

@@ -275,7 +275,7 @@ def test_union_find_cc(gpu, seeded, golden):
         for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
             lab, rep = dg.cc(variant="union_find", loop=loop)
             np.testing.assert_array_equal(lab, ref, err_msg=f"{name} {loop}")
-            assert rep.iterations == 2  # hook launch, compress launch
+            assert rep.iterations == 3  # two hook launches, one compress launch
             lab, rep = dg.cc(variant="heuristic", loop=loop)
             np.testing.assert_array_equal(lab, ref, err_msg=f"{name} heuristic {loop}")
         with pytest.raises(i2.I2Error) as e:
