@@ -1127,34 +1127,57 @@ static int upload_common(i2_graph* g) {
   return st;
 }
 
+// The shape of the CSR is checked on the host; its entries (monotone nindex,
+// nlist in range) on the device right after the copy, before any other kernel
+// reads them: a host pass over nlist costs about as much as copying it. The
+// adjacency and the weights go over two streams (two copy engines).
 int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
   if (!h || !out) return I2_ERR_ARG;
   *out = nullptr;
-  int st = validate_host_csr(h);
-  if (st) return st;
+  if (h->nodes < 1 || h->edges < 0) return I2_ERR_FORMAT;
+  if (!h->nindex || (h->edges > 0 && !h->nlist)) return I2_ERR_ARG;
+  if (h->nindex[0] != 0 || h->nindex[h->nodes] != h->edges) return I2_ERR_FORMAT;
   if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
   i2_graph* g = new i2_graph();
   g->owns = true;
   const size_t nn = (size_t)h->nodes + 1, ne = (size_t)h->edges + 4;
+  cudaStream_t s1 = nullptr, s2 = nullptr;
+  int* bad = nullptr;
+  int hbad = 0;
   cudaError_t e = cudaMalloc(&g->d_nindex, sizeof(int) * nn);
   if (e == cudaSuccess) e = cudaMalloc(&g->d_nlist, sizeof(int) * ne);
   if (e == cudaSuccess && h->eweight) e = cudaMalloc(&g->d_eweight, sizeof(int) * ne);
-  if (e == cudaSuccess) e = cudaMemcpy(g->d_nindex, h->nindex, sizeof(int) * nn, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(g->d_nlist, h->nlist, sizeof(int) * h->edges, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), s1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->d_nindex, h->nindex, sizeof(int) * nn, cudaMemcpyHostToDevice, s1);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g->d_nlist, h->nlist, sizeof(int) * h->edges, cudaMemcpyHostToDevice, s1);
   if (e == cudaSuccess && h->eweight)
-    e = cudaMemcpy(g->d_eweight, h->eweight, sizeof(int) * h->edges, cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    free_graph_state(g);
-    delete g;
-    return cuda_status(e);
-  }
+    e = cudaMemcpyAsync(g->d_eweight, h->eweight, sizeof(int) * h->edges, cudaMemcpyHostToDevice, s2);
   g->g.nodes = h->nodes;
   g->g.edges = h->edges;
   g->g.nindex = g->d_nindex;
   g->g.nlist = g->d_nlist;
   g->g.eweight = g->d_eweight;
-  st = upload_common(g);
+  if (e == cudaSuccess) {
+    k_validate<<<4 * sm_count(), 256, 0, s1>>>(g->g, bad);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s1);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s1);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s2);
+  if (s1) cudaStreamDestroy(s1);
+  if (s2) cudaStreamDestroy(s2);
+  cudaFree(bad);
+  if (e != cudaSuccess || hbad) {
+    cudaGetLastError();
+    free_graph_state(g);
+    delete g;
+    return e != cudaSuccess ? cuda_status(e) : I2_ERR_FORMAT;
+  }
+  int st = upload_common(g);
   if (st) return st;
   *out = g;
   return I2_OK;

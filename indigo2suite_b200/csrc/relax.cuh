@@ -48,10 +48,30 @@ typedef cub::BlockScan<int, kBlock> BlockScanT;
 // keeps the randomly accessed, L2-sized arrays (values, bitmaps, frontier
 // lists, nindex) resident in L2 instead of the streamed lines. On RMAT-22 this
 // measured 3-7% faster for BFS, SSSP and CC than the read-only path.
-// I2_STREAM_LOADS: 0 read-only path without a hint, 1 evict-first (default).
+// I2_STREAM_LOADS: 0 read-only path without a hint, 1 evict-first (default),
+// 2 explicit L2 policies: adjacency evict-first, not allocated in L1.
 #ifndef I2_STREAM_LOADS
 #define I2_STREAM_LOADS 1
 #endif
+#if I2_STREAM_LOADS == 2
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ int ld_adj(const int* p) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;"
+               : "=r"(v) : "l"(p), "l"(l2_evict_first()));
+  return v;
+}
+__device__ __forceinline__ int4 ld_adj(const int4* p) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(l2_evict_first()));
+  return v;
+}
+#else
 template <typename T>
 __device__ __forceinline__ T ld_adj(const T* p) {
 #if I2_STREAM_LOADS
@@ -60,6 +80,7 @@ __device__ __forceinline__ T ld_adj(const T* p) {
   return __ldg(p);
 #endif
 }
+#endif
 
 // Frontier statistics of one thread's pushes; kept in registers and reduced
 // once per block at the end of the launch.
@@ -1090,27 +1111,39 @@ __device__ __forceinline__ int uf_find_fresh(int* p, int x) {
   }
 }
 
-// Called by the whole last block of the first hook launch: the roots of
-// kAfforestSamples vertices spread over the graph, and the root held by a
-// majority of them (Boyer-Moore vote), taken as the largest tree. Any root
-// would keep the result correct; the vote only decides how many vertices the
-// second hook launch can skip.
+// Boyer-Moore majority pairs (candidate, count) merge like single votes: a
+// majority element of the union survives the merge of the parts' pairs.
+__device__ __forceinline__ void vote_merge(int& cand, int& cnt, int c2, int n2) {
+  if (c2 == cand) cnt += n2;
+  else if (n2 > cnt) { cand = c2; cnt = n2 - cnt; }
+  else cnt -= n2;
+}
+
+// Called by the whole last block of the first hook launch (kBlock threads):
+// the roots of kAfforestSamples vertices spread over the graph, and the root
+// held by a majority of them (Boyer-Moore vote, per thread, then merged across
+// lanes and warps), taken as the largest tree. Any root would keep the result
+// correct; the vote only decides how many vertices the second hook launch can
+// skip. Registers and 64 bytes of shared memory: this runs in the epilogue of
+// every relax kernel, whose shared-memory size sets the L1 left to it.
 __device__ __forceinline__ void uf_sample_giant(const Ctx& c) {
-  __shared__ int roots[kAfforestSamples];
+  __shared__ int wc[kBlock / kWarp], wn[kBlock / kWarp];
   const int V = c.g.nodes;
+  int cand = -1, cnt = 0;
   for (int k = threadIdx.x; k < kAfforestSamples; k += blockDim.x)
-    roots[k] = V > 0 ? uf_find_fresh(c.dist, (int)((unsigned)mis_priority(k) % (unsigned)V)) : 0;
+    vote_merge(cand, cnt, V > 0 ? uf_find_fresh(c.dist, (int)((unsigned)mis_priority(k) % (unsigned)V)) : 0, 1);
+  for (int o = 16; o > 0; o >>= 1) {
+    const int c2 = __shfl_down_sync(0xffffffffu, cand, o);
+    const int n2 = __shfl_down_sync(0xffffffffu, cnt, o);
+    vote_merge(cand, cnt, c2, n2);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    wc[threadIdx.x >> 5] = cand;
+    wn[threadIdx.x >> 5] = cnt;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    int cand = -1, cnt = 0;
-    for (int k = 0; k < kAfforestSamples; ++k) {
-      if (cnt == 0) {
-        cand = roots[k];
-        cnt = 1;
-      } else {
-        cnt += roots[k] == cand ? 1 : -1;
-      }
-    }
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) vote_merge(cand, cnt, wc[w], wn[w]);
     c.ctl->uf_giant = cand;
   }
   __syncthreads();

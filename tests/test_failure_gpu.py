@@ -125,3 +125,22 @@ def test_bad_loop_mode_is_refused(gpu):
         dg.bfs(0, loop=3)
     assert e.value.status == _capi.I2_ERR_ARG
     dg.free()
+
+
+def test_malformed_host_graph_rejected_on_upload(gpu):
+    # The upload checks the entries on the device after the copy; a malformed
+    # CSR must still be refused before any traversal reads it.
+    g = i2.gen_er(64, 128, 3)
+    nl = g.nlist.copy()
+    nl[5] = 1000  # out of range
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.upload(i2.ECLGraph(g.nodes, g.edges, g.nindex, nl, g.eweight))
+    assert e.value.status == _capi.I2_ERR_FORMAT
+    ni = g.nindex.copy()
+    ni[3] = ni[4] + 1  # non-monotone
+    with pytest.raises(i2.I2Error) as e:
+        i2.DeviceGraph.upload(i2.ECLGraph(g.nodes, g.edges, ni, g.nlist, g.eweight))
+    assert e.value.status == _capi.I2_ERR_FORMAT
+    dg = i2.DeviceGraph.upload(g)  # and a good one still works
+    assert np.array_equal(dg.bfs(0)[0], __import__("oracle").bfs(g, 0))
+    dg.free()
