@@ -35,8 +35,14 @@ namespace i2 {
 namespace cg = cooperative_groups;
 
 constexpr int kScanItems = kQueue / kBlock;                 // staged entries per thread in a flush
+// Edges per lane of the edge-balanced tile, and the resident blocks per SM its
+// kernels are compiled for (which bounds their registers: 6 -> 40 per thread).
+// Measured on RMAT-22 and a 2048^2 grid (ms, SSSP / BFS / CC on RMAT):
+// 2 edges at 6 blocks 2.65 / 1.12 / 2.21 (default), 4 at 5 blocks 2.80 / 1.14
+// / 2.23, 3 at 5 2.78 / 1.14 / 2.30, 1 at 8 3.11 / 1.24 / 2.39; 2 at 7 or 8
+// blocks and 4 at 6 spill and run 1.2-2x slower.
 #ifndef I2_EB_EDGES
-#define I2_EB_EDGES 4
+#define I2_EB_EDGES 2
 #endif
 constexpr int kEdgesPerThread = I2_EB_EDGES;                // edge-balanced variant
 constexpr int kTileEdges = kBlock * kEdgesPerThread;        // edges per edge-balanced tile
@@ -726,11 +732,8 @@ struct EpiStage {
   int last;
 };
 
-// Minimum resident blocks per SM the edge-balanced kernel is compiled for
-// (bounds its registers: 5 -> 48 per thread). On RMAT-22, 5 measured 10-13%
-// faster than 4 or 6 for BFS, SSSP and CC; 8 edges per lane was slower.
 #ifndef I2_EB_MIN_BLOCKS
-#define I2_EB_MIN_BLOCKS 5
+#define I2_EB_MIN_BLOCKS 6
 #endif
 
 struct EBShared {
