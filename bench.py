@@ -111,6 +111,11 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # wait for its first sample: its start-up queries the device, which
+            # would land inside a short timed region
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 
@@ -270,7 +275,7 @@ def run_ours(args, rank: int, world: int, local: int):
     dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    clocks.start()
+    clocks.start()  # (settles for a moment: starting nvidia-smi queries the device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -529,7 +534,7 @@ def run_batch512(args, rank: int, world: int, local: int):
     torch.cuda.synchronize()
     dist.barrier()
     clocks = Clocks(local)
-    clocks.start()
+    clocks.start()  # (settles for a moment: starting nvidia-smi queries the device)
     t_b = _event_time(torch, stream, batched, args.steps)
     clk = clocks.stop()
     t_p = _event_time(torch, stream, per_graph, max(1, args.steps // 3))
