@@ -510,6 +510,16 @@ def run_batch512(args, rank: int, world: int, local: int):
     b = i2.Batch(graphs)
     per = [i2.DeviceGraph.upload(g) for g in graphs]
     variant = args.variant
+    # the autotuner's committed table (style, blocks per SM, heavy threshold),
+    # applied to the batched and the per-graph runs alike
+    from indigo2suite_b200 import autotune
+
+    tuned = autotune.load()
+    if tuned:
+        variant = tuned["style"]
+        b.tune(heavy_threshold=tuned["heavy_threshold"], blocks_per_sm=tuned["blocks_per_sm"])
+        for g in per:
+            g.tune(heavy_threshold=tuned["heavy_threshold"], blocks_per_sm=tuned["blocks_per_sm"])
     # parity: batched == per-graph, for both algorithms
     for algo in (i2.I2_BFS, i2.I2_SSSP):
         b.run_device(algo, srcs, variant=variant)
@@ -554,6 +564,7 @@ def run_batch512(args, rank: int, world: int, local: int):
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": "batch512_bfs_sssp", "graphs": len(specs), "graphs_this_rank": len(graphs),
                        "nodes_this_rank": V, "edges_this_rank": E, "variant": variant,
+                       "tuning": tuned or "untuned (no indigo2suite_b200/tuning_table.json)",
                        "families": "ER(avg deg 8)/RMAT(ef16)/grid, n log-uniform [1e3,1e6]",
                        "parallelism": f"graphs sharded x{world}", "generation_s": gen_s},
             "batched_ms": 1e3 * t_b, "per_graph_ms": 1e3 * t_p, "per_graph_host_loop_ms": 1e3 * t_h,

@@ -259,6 +259,10 @@ int i2_batch_offsets(const i2_batch* b, long long* voff);
    opts->stream when rep is NULL); i2_batch_result copies it to the host. */
 int i2_batch_run_device(i2_batch* b, int algo, const int* srcs, const i2_opts* opts, i2_report* rep);
 int i2_batch_result(i2_batch* b, int* dist, const i2_opts* opts);
+/* Tuning of the batch's traversals, as i2_graph_tune (no counterpart in the
+   reference; the values come from indigo2suite_b200/tuning_table.json, written
+   by the project's autotuner). */
+int i2_batch_tune(i2_batch* b, int heavy_threshold, int blocks_per_sm, int smem_carveout);
 int i2_batch_free(i2_batch* b);
 
 #ifdef __cplusplus

@@ -356,6 +356,9 @@ class Batch:
             raise I2Error(st, "batch run")
         return [dist[self.voff[k]:self.voff[k + 1]] for k in range(len(self.graphs))], _report(r, st)
 
+    def tune(self, heavy_threshold: int = 0, blocks_per_sm: int = 0, smem_carveout: int = -1) -> None:
+        _check(lib.i2_batch_tune(self._h, heavy_threshold, blocks_per_sm, smem_carveout), "batch tune")
+
     def run_device(self, algo: int, srcs=None, variant="vp_cta", loop=I2_LOOP_GRAPH, stream=None,
                    report: bool = True):
         """Traversal of every graph with results left on the device."""

@@ -119,6 +119,7 @@ SIGNATURES = {
     "i2_batch_offsets": (_I, [_P, C.POINTER(C.c_longlong)]),
     "i2_batch_run_device": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_batch_result": (_I, [_P, _PI, C.POINTER(Opts)]),
+    "i2_batch_tune": (_I, [_P, _I, _I, _I]),
     "i2_batch_free": (_I, [_P]),
 }
 

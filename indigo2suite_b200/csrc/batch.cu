@@ -151,6 +151,11 @@ int i2_batch_result(i2_batch* b, int* dist, const i2_opts* opts) {
   return graph_copy_result(b->g, dist, opts);
 }
 
+int i2_batch_tune(i2_batch* b, int heavy_threshold, int blocks_per_sm, int smem_carveout) {
+  if (!b) return I2_ERR_ARG;
+  return i2_graph_tune(b->g, heavy_threshold, blocks_per_sm, smem_carveout);
+}
+
 int i2_batch_free(i2_batch* b) {
   if (!b) return I2_ERR_ARG;
   i2_graph_free(b->g);

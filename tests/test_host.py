@@ -142,3 +142,19 @@ def test_upload_without_device_is_a_status_not_a_crash():
     with pytest.raises(i2.I2Error) as e:
         i2.DeviceGraph.upload(g)
     assert e.value.status == _capi.I2_ERR_NO_DEVICE
+
+
+def test_autotune_candidates_and_table():
+    from indigo2suite_b200 import autotune
+
+    cands = list(autotune.candidates())
+    assert len(cands) == len(set(cands))
+    assert {c[0] for c in cands} == set(autotune.STYLES)
+    assert {c[1] for c in cands} == set(autotune.BLOCKS_PER_SM)
+    # the heavy threshold is swept only where it matters
+    assert {c[2] for c in cands if c[0] == "vp_cta"} == {4096}
+    assert {c[2] for c in cands if c[0] == "vp_thread"} == set(autotune.HEAVY)
+    assert autotune.load("/nonexistent/table.json") is None
+    if autotune.TABLE_PATH.exists():
+        t = autotune.load()
+        assert t["style"] in autotune.STYLES and t["blocks_per_sm"] in autotune.BLOCKS_PER_SM

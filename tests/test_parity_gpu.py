@@ -304,3 +304,18 @@ def test_switching_style_at_any_iteration(gpu, seeded, name):
                 out, _ = getattr(dg, an)(*src_arg, variant=a, then_variant=b, then_at=k)
                 np.testing.assert_array_equal(out, ref[an], err_msg=f"{name} {an} {a}->{b} at {k}")
     dg.free()
+
+
+def test_batch_tuning_keeps_results(gpu):
+    from indigo2suite_b200 import workloads
+
+    gs = [workloads.build(s) for s in workloads.batch_specs(12, seed=21, nmax=2e4)]
+    srcs = [workloads.source(g) for g in gs]
+    b = i2.Batch(gs)
+    for heavy, bps, style in ((1024, 2, "vp_thread"), (16384, 8, "vp_warp"), (4096, 6, "heuristic")):
+        b.tune(heavy_threshold=heavy, blocks_per_sm=bps)
+        for algo, ref in ((i2.I2_BFS, oracle.bfs), (i2.I2_SSSP, oracle.sssp)):
+            got, _ = b.run(algo, srcs, variant=style)
+            for k, g in enumerate(gs):
+                np.testing.assert_array_equal(got[k], ref(g, srcs[k]), err_msg=f"{style} {bps} {heavy} graph {k}")
+    b.free()
