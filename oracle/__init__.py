@@ -269,6 +269,27 @@ def certify_cc(g, label: np.ndarray) -> str | None:
     return None
 
 
+def certify_mis(g, status: np.ndarray) -> str | None:
+    """The checks of the reference MIS harness's verifier
+    (include/mis_vertex_cuda.h:80-98): every vertex decided, no two adjacent
+    vertices in the set, and every excluded vertex has a neighbour in the set.
+    Returns None when they hold."""
+    st = np.asarray(status)
+    if not np.isin(st, (1, 2)).all():
+        return "undecided vertex"
+    deg = np.diff(np.asarray(g.nindex, np.int64))
+    u = np.repeat(np.arange(g.nodes, dtype=np.int64), deg)
+    inn = st == 1
+    nbr_in = inn[np.asarray(g.nlist, np.int64)]
+    if (inn[u] & nbr_in).any():
+        return "adjacent vertices in the set"
+    covered = np.zeros(g.nodes, bool)
+    covered[u[nbr_in]] = True
+    if not (inn | covered).all():
+        return "set is not maximal"
+    return None
+
+
 # ---------------------------------------------------------------------------
 # One call of a reference CPU host driver (oracle/_ref/libref_cpu_<name>.so).
 

@@ -52,3 +52,14 @@ def test_rmat22_bfs_and_cc(gpu, rmat22):
         lab = dg.cc(variant=v)[0]
         np.testing.assert_array_equal(lab, lab_ref, err_msg=v)
     assert oracle.certify_cc(g, lab) is None
+
+
+def test_rmat22_union_find_learned_and_mis(gpu, rmat22):
+    dg, g = rmat22
+    lab_ref = oracle.cc(g)
+    for v in ("union_find", "learned"):
+        lab, rep = dg.cc(variant=v)
+        np.testing.assert_array_equal(lab, lab_ref, err_msg=v)
+    st, rep = dg.mis()
+    np.testing.assert_array_equal(st, oracle.mis(g))
+    assert oracle.certify_mis(g, st) is None

@@ -132,6 +132,22 @@ def test_mis_oracle_is_the_greedy_set(unsigned):
                 assert any(st[u] == 1 for u in nb)
 
 
+def test_mis_certificate_accepts_oracle_and_rejects_planted_mistakes():
+    g = i2.gen_rmat(12, 8, seed=4)
+    st = oracle.mis(g)
+    assert oracle.certify_mis(g, st) is None
+    v_in = int(np.flatnonzero((st == 1) & (g.degrees() > 0))[0])
+    bad = st.copy()
+    bad[g.nlist[g.nindex[v_in]]] = 1  # a neighbour of a vertex in the set
+    assert oracle.certify_mis(g, bad) == "adjacent vertices in the set"
+    bad = st.copy()
+    bad[v_in] = 2  # it has no neighbour in the set
+    assert oracle.certify_mis(g, bad) == "set is not maximal"
+    bad = st.copy()
+    bad[0] = 0
+    assert oracle.certify_mis(g, bad) == "undecided vertex"
+
+
 @pytest.mark.skipif(not oracle.have_ref(), reason="reference programs not built")
 def test_mis_oracle_matches_reference_cpu_program():
     # The reference's C++ MIS codes compare priorities as unsigned int; the
