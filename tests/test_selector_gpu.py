@@ -40,18 +40,21 @@ def test_learned_results_are_bit_exact(params):
 
 def test_learned_beats_the_fixed_heuristic_on_held_out_graphs(params):
     # What the trained network adds over the fixed rule: on high-diameter
-    # graphs it moves BFS and SSSP iterations to the pull and topology styles
-    # (the rule keeps the push there); held-out grids of 2^18 and 2^20 vertices
-    # measured 0.75-0.89x the rule's time. For CC both selectors take
-    # union-find, and on RMAT/ER graphs they are at par, so those cases say
-    # nothing either way.
-    ratios = []
-    for spec in (S.GraphSpec("grid", 18, 8104), S.GraphSpec("grid", 20, 8105)):
+    # graphs it moves BFS and SSSP iterations to the pull and topology styles,
+    # where the rule keeps the push. On held-out 2^18-vertex grids (three
+    # seeds, two B200 boxes) that measured 0.89-0.99x the rule's time; on
+    # 2^20-vertex grids the two are at par (0.99-1.06x), and on RMAT/ER graphs
+    # and for CC (both take union-find) they are at par too, so those cases
+    # are only checked for not losing much.
+    gains, par = [], []
+    for spec in (S.GraphSpec("grid", 18, 8104), S.GraphSpec("grid", 18, 8106), S.GraphSpec("grid", 20, 8105)):
         g = spec.build()
         dg = i2.DeviceGraph.upload(g)
         src = int(np.argmax(g.degrees()))
         for algo in (i2.I2_BFS, i2.I2_SSSP):
-            ratios.append(_median_ms(dg, algo, src, "learned", 7) / _median_ms(dg, algo, src, "heuristic", 7))
+            r = _median_ms(dg, algo, src, "learned", 7) / _median_ms(dg, algo, src, "heuristic", 7)
+            (gains if spec.scale == 18 else par).append(r)
         dg.free()
-    geo = math.exp(sum(math.log(r) for r in ratios) / len(ratios))
-    assert geo < 0.98, ratios
+    geo = math.exp(sum(math.log(r) for r in gains) / len(gains))
+    assert geo < 0.98, gains
+    assert max(par) < 1.15, par
