@@ -189,6 +189,11 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_
 /* Give the graph the reference's synthetic weights when it has none (on the device). */
 int i2_graph_synth_weights(i2_graph* g);
 int i2_graph_free(i2_graph* g);
+/* Device memory of freed graphs stays reserved in the engine's pool on its
+   device, so the next upload or workspace reuses it without a cudaMalloc;
+   this hands the unused part of the current device's pool back to the driver
+   (for another allocator in the same process). Waits for the device. */
+int i2_trim_device_memory(void);
 
 /* ---- traversals (replace GPU<alg>_<vertex|edge>) ----
    dist/label are HOST arrays of g.nodes ints, filled before return. */

@@ -67,6 +67,12 @@ def device_count() -> int:
     return int(lib.i2_device_count())
 
 
+def trim_device_memory() -> None:
+    """Hand the device memory that freed graphs left reserved in the engine's
+    pool (current device) back to the driver."""
+    _check(lib.i2_trim_device_memory(), "trim device memory")
+
+
 def variant_id(v) -> int:
     if isinstance(v, (int, np.integer)):
         return int(v)

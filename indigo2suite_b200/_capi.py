@@ -101,6 +101,7 @@ SIGNATURES = {
     "i2_graph_tune": (_I, [_P, _I, _I, _I]),
     "i2_gen_rmat_n": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I, _PG]),
     "i2_graph_free": (_I, [_P]),
+    "i2_trim_device_memory": (_I, []),
     "i2_bfs": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_sssp": (_I, [_P, _I, _PI, C.POINTER(Opts), C.POINTER(Report)]),
     "i2_cc": (_I, [_P, _PI, C.POINTER(Opts), C.POINTER(Report)]),

@@ -50,9 +50,9 @@ int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out) {
   if (V > 0x7ffffffeLL || E > 0x7ffffffbLL) return I2_ERR_OVERFLOW;
   if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
   int *nindex = nullptr, *nlist = nullptr, *w = nullptr;
-  cudaError_t e = cudaMalloc(&nindex, sizeof(int) * (V + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&nlist, sizeof(int) * (E + 4));
-  if (e == cudaSuccess && weighted) e = cudaMalloc(&w, sizeof(int) * (E + 4));
+  cudaError_t e = dev_alloc(&nindex, sizeof(int) * (V + 1));
+  if (e == cudaSuccess) e = dev_alloc(&nlist, sizeof(int) * (E + 4));
+  if (e == cudaSuccess && weighted) e = dev_alloc(&w, sizeof(int) * (E + 4));
   i2_batch* b = new i2_batch();
   b->n = n;
   long long vo = 0, eo = 0;
@@ -83,9 +83,9 @@ int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out) {
   if (e != cudaSuccess) {
     const bool bad_input = e == cudaErrorInvalidValue;
     cudaGetLastError();
-    cudaFree(nindex);
-    cudaFree(nlist);
-    cudaFree(w);
+    dev_free(nindex);
+    dev_free(nlist);
+    dev_free(w);
     delete b;
     return bad_input ? I2_ERR_FORMAT : cuda_status(e);
   }

@@ -461,6 +461,104 @@ struct i2_graph {
 
 namespace i2 {
 
+// ---------------------------------------------------------------------------
+// Device memory pool and pinned control blocks.
+
+namespace {
+struct DevPool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t s = nullptr;  // allocations and frees are ordered on it
+};
+std::mutex g_pool_mu;
+DevPool g_pools[64];
+std::mutex g_ctl_mu;
+std::vector<Ctl*> g_ctl_free;  // pinned host control blocks of freed graphs
+}  // namespace
+
+static DevPool* dev_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  DevPool& p = g_pools[dev];
+  if (!p.pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t s = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long keep = ~0ull;  // never hand reserved memory back on its own
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      cudaMemPoolDestroy(pool);
+      return nullptr;
+    }
+    p.pool = pool;
+    p.s = s;
+  }
+  return &p;
+}
+
+cudaError_t dev_alloc_bytes(void** ptr, size_t bytes) {
+  *ptr = nullptr;
+  DevPool* p = dev_pool();
+  if (!p) return cudaErrorInitializationError;
+  cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, p->pool, p->s);
+  if (e == cudaErrorMemoryAllocation) {
+    // Reserved but unused blocks may be too fragmented to serve the request:
+    // hand them back and try once more.
+    cudaGetLastError();
+    cudaStreamSynchronize(p->s);
+    cudaMemPoolTrimTo(p->pool, 0);
+    e = cudaMallocFromPoolAsync(ptr, bytes, p->pool, p->s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->s);  // usable by every stream from here
+  if (e != cudaSuccess) *ptr = nullptr;
+  return e;
+}
+
+void dev_free(void* ptr) {
+  if (!ptr) return;
+  DevPool* p = dev_pool();
+  if (!p) return;
+  cudaDeviceSynchronize();
+  cudaFreeAsync(ptr, p->s);
+}
+
+static int trim_pool() {
+  DevPool* p = dev_pool();
+  if (!p) return I2_ERR_NO_DEVICE;
+  I2_CK(cudaStreamSynchronize(p->s));
+  I2_CK(cudaMemPoolTrimTo(p->pool, 0));
+  return I2_OK;
+}
+
+static cudaError_t ctl_host_get(Ctl** out) {
+  {
+    std::lock_guard<std::mutex> lk(g_ctl_mu);
+    if (!g_ctl_free.empty()) {
+      *out = g_ctl_free.back();
+      g_ctl_free.pop_back();
+      return cudaSuccess;
+    }
+  }
+  return cudaMallocHost(out, sizeof(Ctl));
+}
+
+static void ctl_host_put(Ctl* c) {
+  if (!c) return;
+  std::lock_guard<std::mutex> lk(g_ctl_mu);
+  g_ctl_free.push_back(c);
+}
+
 static void drop_execs(i2_graph* g) {
   for (auto& kv : g->execs) cudaGraphExecDestroy(kv.second.ex);
   g->execs.clear();
@@ -470,41 +568,41 @@ static void free_graph_state(i2_graph* g) {
   drop_execs(g);
   for (auto gr : g->graphs) cudaGraphDestroy(gr);
   g->graphs.clear();
-  cudaFree(g->dist);
+  dev_free(g->dist);
   for (int k = 0; k < 3; ++k) {
-    cudaFree(g->wl[k]);
-    cudaFree(g->woff[k]);
-    cudaFree(g->hwl[k]);
-    cudaFree(g->htoff[k]);
+    dev_free(g->wl[k]);
+    dev_free(g->woff[k]);
+    dev_free(g->hwl[k]);
+    dev_free(g->htoff[k]);
   }
-  cudaFree(g->bm[0]);
-  cudaFree(g->pile[0]);
-  cudaFree(g->pile[1]);
-  cudaFree(g->ctl);
-  cudaFree(g->recs);
-  cudaFree(g->srcs);
-  cudaFree(g->reach);
-  cudaFree(g->snap_dist);
-  cudaFree(g->snap_bm);
-  cudaFree(g->snap_wl);
-  cudaFree(g->snap_hwl);
-  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  dev_free(g->bm[0]);
+  dev_free(g->pile[0]);
+  dev_free(g->pile[1]);
+  dev_free(g->ctl);
+  dev_free(g->recs);
+  dev_free(g->srcs);
+  dev_free(g->reach);
+  dev_free(g->snap_dist);
+  dev_free(g->snap_bm);
+  dev_free(g->snap_wl);
+  dev_free(g->snap_hwl);
+  if (g->h_ctl) ctl_host_put(g->h_ctl);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   if (g->ev2) cudaEventDestroy(g->ev2);
   if (g->ev3) cudaEventDestroy(g->ev3);
   if (g->stream) cudaStreamDestroy(g->stream);
-  cudaFree(g->d_sp);
+  dev_free(g->d_sp);
   if (g->owns) {
-    cudaFree(g->d_nindex);
-    cudaFree(g->d_nlist);
+    dev_free(g->d_nindex);
+    dev_free(g->d_nlist);
   }
-  if (g->owns || g->owns_weights) cudaFree(g->d_eweight);
+  if (g->owns || g->owns_weights) dev_free(g->d_eweight);
 }
 
 static int compute_stats(i2_graph* g) {
   DevStats* st = nullptr;
-  I2_CK(cudaMalloc(&st, sizeof(DevStats)));
+  I2_CK(dev_alloc(&st, sizeof(DevStats)));
   DevStats h{};
   h.wmin = INT_MAX;
   cudaMemcpy(st, &h, sizeof(h), cudaMemcpyHostToDevice);
@@ -513,7 +611,7 @@ static int compute_stats(i2_graph* g) {
   cudaStreamSynchronize(g->stream);
   cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost);
   cudaError_t e = cudaGetLastError();
-  cudaFree(st);
+  dev_free(st);
   if (e != cudaSuccess) return cuda_status(e);
   GStats& s = g->gs;
   s.nodes = g->g.nodes;
@@ -537,7 +635,7 @@ static int finish_setup(i2_graph* g) {
   I2_CK(cudaEventCreate(&g->ev1));
   I2_CK(cudaEventCreate(&g->ev2));
   I2_CK(cudaEventCreate(&g->ev3));
-  I2_CK(cudaMallocHost(&g->h_ctl, sizeof(Ctl)));
+  I2_CK(ctl_host_get(&g->h_ctl));
   g->g.vec_ok = ((((uintptr_t)g->g.nlist) & 15) == 0 && (((uintptr_t)g->g.eweight) & 15) == 0) ? 1 : 0;
   return compute_stats(g);
 }
@@ -546,35 +644,35 @@ static int ensure_workspace(i2_graph* g) {
   if (g->ws_ready) return I2_OK;
   const long long V = g->g.nodes;
   g->bm_words = (int)((V + 31) / 32);
-  I2_CK(cudaMalloc(&g->dist, sizeof(int) * V));
+  I2_CK(dev_alloc(&g->dist, sizeof(int) * V));
   for (int k = 0; k < 3; ++k) {
-    I2_CK(cudaMalloc(&g->wl[k], sizeof(int) * V));
-    I2_CK(cudaMalloc(&g->woff[k], sizeof(unsigned) * V));
-    I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
-    I2_CK(cudaMalloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
+    I2_CK(dev_alloc(&g->wl[k], sizeof(int) * V));
+    I2_CK(dev_alloc(&g->woff[k], sizeof(unsigned) * V));
+    I2_CK(dev_alloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+    I2_CK(dev_alloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
   }
   unsigned* bm = nullptr;
-  I2_CK(cudaMalloc(&bm, sizeof(unsigned) * 4ull * g->bm_words));
+  I2_CK(dev_alloc(&bm, sizeof(unsigned) * 4ull * g->bm_words));
   for (int k = 0; k < 3; ++k) g->bm[k] = bm + (size_t)k * g->bm_words;
   g->fbm = bm + 3ull * g->bm_words;
-  I2_CK(cudaMalloc(&g->ctl, sizeof(Ctl)));
+  I2_CK(dev_alloc(&g->ctl, sizeof(Ctl)));
   g->rec_cap = (int)std::min<long long>(V + 2, 1 << 16);
-  I2_CK(cudaMalloc(&g->recs, sizeof(IterRec) * g->rec_cap));
-  I2_CK(cudaMalloc(&g->reach, sizeof(unsigned long long) * 2));
+  I2_CK(dev_alloc(&g->recs, sizeof(IterRec) * g->rec_cap));
+  I2_CK(dev_alloc(&g->reach, sizeof(unsigned long long) * 2));
   g->ws_ready = true;
   return I2_OK;
 }
 
 static int ensure_piles(i2_graph* g) {
   if (g->pile[0]) return I2_OK;
-  for (int k = 0; k < 2; ++k) I2_CK(cudaMalloc(&g->pile[k], sizeof(int) * ((size_t)g->g.nodes + 1)));
+  for (int k = 0; k < 2; ++k) I2_CK(dev_alloc(&g->pile[k], sizeof(int) * ((size_t)g->g.nodes + 1)));
   drop_execs(g);  // graphs bake the context
   return I2_OK;
 }
 
 static int ensure_sp(i2_graph* g) {
   if (g->d_sp) return I2_OK;
-  I2_CK(cudaMalloc(&g->d_sp, sizeof(int) * ((size_t)g->g.edges + 4)));
+  I2_CK(dev_alloc(&g->d_sp, sizeof(int) * ((size_t)g->g.edges + 4)));
   k_build_sp<<<8 * sm_count(), 256, 0, g->stream>>>(g->g, g->d_sp);
   I2_CK(cudaStreamSynchronize(g->stream));
   g->g.sp = g->d_sp;
@@ -588,7 +686,7 @@ static int ensure_symmetry(i2_graph* g) {
   int st = ensure_sp(g);
   if (st) return st;
   DevStats* d = nullptr;
-  I2_CK(cudaMalloc(&d, sizeof(DevStats)));
+  I2_CK(dev_alloc(&d, sizeof(DevStats)));
   DevStats h{};
   cudaMemcpy(d, &h, sizeof(h), cudaMemcpyHostToDevice);
   const int grid = 8 * sm_count();
@@ -601,7 +699,7 @@ static int ensure_symmetry(i2_graph* g) {
     cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
   }
   cudaError_t e = cudaGetLastError();
-  cudaFree(d);
+  dev_free(d);
   if (e != cudaSuccess) return cuda_status(e);
   g->gs.symmetric = (!h.unsorted && !h.asym) ? 1 : 0;
   drop_execs(g);  // graphs bake the statistics into their arguments
@@ -903,9 +1001,9 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     for (int j = 0; j < nsrc; ++j)
       if (srcs_host[j] < 0 || srcs_host[j] >= g->g.nodes) return I2_ERR_ARG;
     if (g->srcs_cap < nsrc) {
-      cudaFree(g->srcs);
+      dev_free(g->srcs);
       g->srcs = nullptr;
-      I2_CK(cudaMalloc(&g->srcs, sizeof(int) * nsrc));
+      I2_CK(dev_alloc(&g->srcs, sizeof(int) * nsrc));
       g->srcs_cap = nsrc;
       // graphs bake the source pointer: rebuild them
       drop_execs(g);
@@ -994,8 +1092,8 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
   if (st) return st;
   const long long V = g->g.nodes;
   if (!g->snap_dist) {
-    I2_CK(cudaMalloc(&g->snap_dist, sizeof(int) * V));
-    I2_CK(cudaMalloc(&g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words));
+    I2_CK(dev_alloc(&g->snap_dist, sizeof(int) * V));
+    I2_CK(dev_alloc(&g->snap_bm, sizeof(unsigned) * 3ull * g->bm_words));
   }
   cudaStream_t s = g->stream;
   const int mode = follow == I2_AUTO_LEARNED ? 2 : (follow < 0 ? 1 : 0);
@@ -1144,10 +1242,10 @@ int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
   cudaStream_t s1 = nullptr, s2 = nullptr;
   int* bad = nullptr;
   int hbad = 0;
-  cudaError_t e = cudaMalloc(&g->d_nindex, sizeof(int) * nn);
-  if (e == cudaSuccess) e = cudaMalloc(&g->d_nlist, sizeof(int) * ne);
-  if (e == cudaSuccess && h->eweight) e = cudaMalloc(&g->d_eweight, sizeof(int) * ne);
-  if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int));
+  cudaError_t e = dev_alloc(&g->d_nindex, sizeof(int) * nn);
+  if (e == cudaSuccess) e = dev_alloc(&g->d_nlist, sizeof(int) * ne);
+  if (e == cudaSuccess && h->eweight) e = dev_alloc(&g->d_eweight, sizeof(int) * ne);
+  if (e == cudaSuccess) e = dev_alloc(&bad, sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), s1);
@@ -1170,7 +1268,7 @@ int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s2);
   if (s1) cudaStreamDestroy(s1);
   if (s2) cudaStreamDestroy(s2);
-  cudaFree(bad);
+  dev_free(bad);
   if (e != cudaSuccess || hbad) {
     cudaGetLastError();
     free_graph_state(g);
@@ -1236,13 +1334,13 @@ int i2_graph_wrap_device(const i2_eclgraph* d, i2_graph** out) {
   // Validate before any kernel indexes through the arrays.
   int* bad = nullptr;
   int hbad = 0;
-  cudaError_t e = cudaMalloc(&bad, sizeof(int));
+  cudaError_t e = dev_alloc(&bad, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(bad, 0, sizeof(int));
   if (e == cudaSuccess) {
     k_validate<<<4 * sm_count(), 256>>>(g->g, bad);
     e = cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost);
   }
-  cudaFree(bad);
+  dev_free(bad);
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete g;
@@ -1320,8 +1418,8 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_
     g->heavy = std::max(32, heavy_threshold);
     // the heavy lists are sized by the number of heavy vertices
     for (int k = 0; k < 3; ++k) {
-      cudaFree(g->hwl[k]);
-      cudaFree(g->htoff[k]);
+      dev_free(g->hwl[k]);
+      dev_free(g->htoff[k]);
       g->hwl[k] = nullptr;
       g->htoff[k] = nullptr;
     }
@@ -1329,8 +1427,8 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_
     if (st) return st;
     if (g->ws_ready)
       for (int k = 0; k < 3; ++k) {
-        I2_CK(cudaMalloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
-        I2_CK(cudaMalloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
+        I2_CK(dev_alloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
+        I2_CK(dev_alloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
       }
   }
   return I2_OK;
@@ -1341,7 +1439,7 @@ int i2_graph_synth_weights(i2_graph* g) {
   if (g->g.eweight) return I2_OK;
   I2_CK(cudaSetDevice(g->device));
   int* w = nullptr;
-  I2_CK(cudaMalloc(&w, sizeof(int) * ((size_t)g->g.edges + 4)));
+  I2_CK(dev_alloc(&w, sizeof(int) * ((size_t)g->g.edges + 4)));
   k_synth_weights<<<8 * sm_count(), 256, 0, g->stream>>>(g->g, w);
   I2_CK(cudaStreamSynchronize(g->stream));
   g->d_eweight = w;
@@ -1359,6 +1457,11 @@ int i2_graph_free(i2_graph* g) {
   free_graph_state(g);
   delete g;
   return I2_OK;
+}
+
+int i2_trim_device_memory(void) {
+  if (i2_device_count() < 1) return I2_ERR_NO_DEVICE;
+  return trim_pool();
 }
 
 static int run_host_out(i2_graph* g, int algo, int src, int* out, const i2_opts* opts, i2_report* rep) {

@@ -29,4 +29,19 @@ int graph_adopt(int nodes, int edges, int* d_nindex, int* d_nlist, int* d_eweigh
 // Copy the last traversal's values to a host array of g.nodes ints.
 int graph_copy_result(i2_graph* g, int* host_out, const i2_opts* opts);
 
+// Device memory of graphs (CSR arrays, workspaces, scratch) comes from one
+// stream-ordered pool per device that keeps freed blocks reserved: a graph
+// uploaded after another was freed reuses that memory instead of paying a
+// cudaMalloc and a cudaFree (a change of the device's mappings, milliseconds
+// per GB) for every array. dev_alloc returns memory every stream may use;
+// dev_free keeps cudaFree's contract (the device finishes its work before the
+// block goes back to the pool). Every pointer dev_free gets must come from
+// dev_alloc.
+cudaError_t dev_alloc_bytes(void** p, size_t bytes);
+void dev_free(void* p);
+template <class T>
+inline cudaError_t dev_alloc(T** p, size_t bytes) {
+  return dev_alloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+
 }  // namespace i2

@@ -74,16 +74,16 @@ extern "C" int i2_graph_generate_rmat(int scale, int edge_factor, double a, doub
   size_t tb = 0, tb2 = 0;
   long long num = 0, E = 0;
   unsigned long long last = 0;
-  cudaError_t e = cudaMalloc(&k0, sizeof(unsigned long long) * nkeys);
-  if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(unsigned long long) * nkeys);
-  if (e == cudaSuccess) e = cudaMalloc(&d_num, sizeof(long long));
+  cudaError_t e = dev_alloc(&k0, sizeof(unsigned long long) * nkeys);
+  if (e == cudaSuccess) e = dev_alloc(&k1, sizeof(unsigned long long) * nkeys);
+  if (e == cudaSuccess) e = dev_alloc(&d_num, sizeof(long long));
   if (e != cudaSuccess) goto done;
   k_rmat_keys<<<4096, 256>>>(seed, scale, t, p, samples, (int)n, k0);
   {
     cub::DoubleBuffer<unsigned long long> db(k0, k1);
     e = cub::DeviceRadixSort::SortKeys(nullptr, tb, db, nkeys);
     if (e == cudaSuccess) e = cub::DeviceSelect::Unique(nullptr, tb2, k0, k1, d_num, nkeys);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max(tb, tb2));
+    if (e == cudaSuccess) e = dev_alloc(&tmp, std::max(tb, tb2));
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(tmp, tb, db, nkeys);
     if (e != cudaSuccess) goto done;
     unsigned long long* sorted = db.Current();
@@ -98,26 +98,26 @@ extern "C" int i2_graph_generate_rmat(int scale, int edge_factor, double a, doub
       st = I2_ERR_OVERFLOW;
       goto done;
     }
-    e = cudaMalloc(&nindex, sizeof(int) * (n + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&nlist, sizeof(int) * (E + 4));
-    if (e == cudaSuccess && weighted) e = cudaMalloc(&w, sizeof(int) * (E + 4));
+    e = dev_alloc(&nindex, sizeof(int) * (n + 1));
+    if (e == cudaSuccess) e = dev_alloc(&nlist, sizeof(int) * (E + 4));
+    if (e == cudaSuccess && weighted) e = dev_alloc(&w, sizeof(int) * (E + 4));
     if (e != cudaSuccess) goto done;
     k_cut_csr<<<4096, 256>>>(other, E, (int)n, seed, weighted, nindex, nlist, w);
     e = cudaDeviceSynchronize();
   }
 done:
-  cudaFree(k0);
-  cudaFree(k1);
-  cudaFree(d_num);
-  cudaFree(tmp);
+  dev_free(k0);
+  dev_free(k1);
+  dev_free(d_num);
+  dev_free(tmp);
   if (st == I2_OK && e != cudaSuccess) {
     cudaGetLastError();
     st = cuda_status(e);
   }
   if (st != I2_OK) {
-    cudaFree(nindex);
-    cudaFree(nlist);
-    cudaFree(w);
+    dev_free(nindex);
+    dev_free(nlist);
+    dev_free(w);
     return st;
   }
   return graph_adopt((int)n, (int)E, nindex, nlist, w, out);

@@ -158,3 +158,11 @@ def test_autotune_candidates_and_table():
     if autotune.TABLE_PATH.exists():
         t = autotune.load()
         assert t["style"] in autotune.STYLES and t["blocks_per_sm"] in autotune.BLOCKS_PER_SM
+
+
+def test_trim_without_device_is_a_status():
+    if i2.device_count() > 0:
+        pytest.skip("a device is present")
+    with pytest.raises(i2.I2Error) as e:
+        i2.trim_device_memory()
+    assert e.value.status == _capi.I2_ERR_NO_DEVICE

@@ -319,3 +319,24 @@ def test_batch_tuning_keeps_results(gpu):
             for k, g in enumerate(gs):
                 np.testing.assert_array_equal(got[k], ref(g, srcs[k]), err_msg=f"{style} {bps} {heavy} graph {k}")
     b.free()
+
+
+def test_pooled_memory_reuse_and_trim(gpu):
+    # Graphs freed and uploaded again reuse the pool's memory; results do not
+    # depend on what the reused blocks held, and trimming the pool leaves
+    # later uploads working.
+    g1 = i2.gen_rmat(14, 16, seed=41)
+    g2 = i2.gen_er(30000, 120000, 42)
+    src1, src2 = int(np.argmax(g1.degrees())), int(np.argmax(g2.degrees()))
+    ref1, ref2 = oracle.sssp(g1, src1), oracle.bfs(g2, src2)
+    for k in range(3):
+        dg = i2.DeviceGraph.upload(g1)
+        np.testing.assert_array_equal(dg.sssp(src1)[0], ref1)
+        dg.free()
+        dg = i2.DeviceGraph.upload(g2)
+        np.testing.assert_array_equal(dg.bfs(src2, variant="heuristic")[0], ref2)
+        np.testing.assert_array_equal(dg.cc(variant="union_find")[0], oracle.cc(g2))
+        dg.free()
+        if k == 1:
+            i2.trim_device_memory()
+    i2.trim_device_memory()
