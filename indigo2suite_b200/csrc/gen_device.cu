@@ -74,16 +74,16 @@ extern "C" int i2_graph_generate_rmat(int scale, int edge_factor, double a, doub
   size_t tb = 0, tb2 = 0;
   long long num = 0, E = 0;
   unsigned long long last = 0;
-  cudaError_t e = dev_alloc(&k0, sizeof(unsigned long long) * nkeys);
-  if (e == cudaSuccess) e = dev_alloc(&k1, sizeof(unsigned long long) * nkeys);
-  if (e == cudaSuccess) e = dev_alloc(&d_num, sizeof(long long));
+  cudaError_t e = cudaMalloc(&k0, sizeof(unsigned long long) * nkeys);
+  if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(unsigned long long) * nkeys);
+  if (e == cudaSuccess) e = cudaMalloc(&d_num, sizeof(long long));
   if (e != cudaSuccess) goto done;
   k_rmat_keys<<<4096, 256>>>(seed, scale, t, p, samples, (int)n, k0);
   {
     cub::DoubleBuffer<unsigned long long> db(k0, k1);
     e = cub::DeviceRadixSort::SortKeys(nullptr, tb, db, nkeys);
     if (e == cudaSuccess) e = cub::DeviceSelect::Unique(nullptr, tb2, k0, k1, d_num, nkeys);
-    if (e == cudaSuccess) e = dev_alloc(&tmp, std::max(tb, tb2));
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max(tb, tb2));
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(tmp, tb, db, nkeys);
     if (e != cudaSuccess) goto done;
     unsigned long long* sorted = db.Current();
@@ -106,10 +106,12 @@ extern "C" int i2_graph_generate_rmat(int scale, int edge_factor, double a, doub
     e = cudaDeviceSynchronize();
   }
 done:
-  dev_free(k0);
-  dev_free(k1);
-  dev_free(d_num);
-  dev_free(tmp);
+  // the sort's scratch is transient: plain allocations, returned at once;
+  // the graph's arrays come from the engine's pool
+  cudaFree(k0);
+  cudaFree(k1);
+  cudaFree(d_num);
+  cudaFree(tmp);
   if (st == I2_OK && e != cudaSuccess) {
     cudaGetLastError();
     st = cuda_status(e);
