@@ -317,6 +317,7 @@ def run_ours(args, rank: int, world: int, local: int):
         if tr.get("kernel") == roofline["kernel"]:  # a capture of this configuration's kernel
             roofline["traffic"] = tr.get("dram_bytes_per_launch")
             roofline["traffic_note"] = tr.get("note")
+            roofline["traffic_captured_with"] = tr.get("captured_with")
 
     # the other styles and the selectors (a few steps each)
     styles = {}
