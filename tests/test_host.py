@@ -158,6 +158,14 @@ def test_autotune_candidates_and_table():
     if autotune.TABLE_PATH.exists():
         t = autotune.load()
         assert t["style"] in autotune.STYLES and t["blocks_per_sm"] in autotune.BLOCKS_PER_SM
+        # the committed table covers every candidate and chose the fastest
+        import json
+        table = json.loads(autotune.TABLE_PATH.read_text())
+        rows = table["candidates"]
+        assert {(r["style"], r["blocks_per_sm"], r["heavy_threshold"]) for r in rows} == set(cands)
+        best = min(rows, key=lambda r: r["total_ms"])
+        assert (best["style"], best["blocks_per_sm"], best["heavy_threshold"]) == \
+            (t["style"], t["blocks_per_sm"], t["heavy_threshold"])
 
 
 def test_trim_without_device_is_a_status():
