@@ -205,33 +205,55 @@ def ref_cuda_baseline(g, src: int) -> dict:
             "sample": "full workload graph; the program's own runtime print (device loop, verification off)"}
 
 
+def graph_digest(g) -> str:
+    """First 16 hex digits of SHA-256 over nindex, nlist and eweight: both arms
+    put it in `config`, so equal configs mean the same graph."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a in (g.nindex, g.nlist, g.eweight):
+        h.update(np.ascontiguousarray(a, np.int32)[: len(a)].tobytes())
+    return h.hexdigest()[:16]
+
+
+def bench_config(args, g, world: int) -> dict:
+    """The benchmark line's `config`, identical in both arms."""
+    return dict(WORKLOAD, variant=args.variant, edges=g.edges, nodes=g.nodes, graph_sha16=graph_digest(g),
+                parallelism=f"replicas x{world}", loop=args.loop,
+                near_far_step=args.delta if args.delta > 0 else "off")
+
+
 def run_reference(args, rank: int, world: int):
+    """The reference's own CPU SSSP on the benchmark graph. The graph comes from
+    the oracle's independent C generator (oracle/graphgen.c, the same CSR as the
+    engine's generators), so this arm loads no engine code."""
     if rank != 0:
         return
     import oracle
 
-    import indigo2suite_b200 as i2  # host generator only (same CSR as the device generator)
-
     if not (oracle.REF_OUT / "libref_cpu_sssp_vertex_cpp.so").exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference CPU programs)"}))
         return
-    g = i2.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
+    g = oracle.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
     src = graph_source(g)
     threads = os.cpu_count() or 1
+    prog = "sssp_vertex_cpp"
     for _ in range(args.warmup):
-        oracle.ref_cpu_run("sssp_vertex_cpp", g, src, threads)
+        oracle.ref_cpu_run(prog, g, src, threads)
     ts = []
     for _ in range(args.steps):
-        t, _ = oracle.ref_cpu_run("sssp_vertex_cpp", g, src, threads)
+        t, _ = oracle.ref_cpu_run(prog, g, src, threads)
         ts.append(t)
     total = sum(ts)
     value = 1e-9 * g.edges * args.steps / total
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "config": dict(WORKLOAD, reference_program="sssp_vertex_cpp"),
+            "data": "synthetic", "config": bench_config(args, g, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": "full workload graph, one traversal per step"},
+                             "program": prog + " (codes/cpp/sssp-cpp/SSSP_CPP_V_Data_Push_..._NonDup.cpp, "
+                                               "built unchanged)",
+                             "sample": "full workload graph, one traversal per step, the program's own timer"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -397,8 +419,7 @@ def run_ours(args, rank: int, world: int, local: int):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": dict(WORKLOAD, variant=variant, edges=E, nodes=V, parallelism=f"replicas x{world}",
-                           loop=args.loop, near_far_step=delta if delta > 0 else "off"),
+            "config": bench_config(args, host, world),
             "roofline": roofline, "cpu_baseline": cpu, "reference_cuda": ref_cuda, "e2e": e2e,
             "e2e_query": e2e_query,
             "gpu_launches": launches, "clocks": clk,

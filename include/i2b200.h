@@ -247,11 +247,16 @@ int i2_mlp_predict(const float* params, const float* X, int n, int allowed_mask,
    array inside the library (about 3 MB, held on every GPU that loads the
    library until exit), so graphs above 131072 vertices return I2_ERR_CAPACITY.
    Style: edge-balanced push, host-driven loop on `stream` (NULL: legacy
-   stream). The first call on each device looks up the scratch's device
-   address; make that first call before any stream capture. All calls share the
-   one scratch: calls that overlap on the GPU (other streams, other host
-   threads) race and must be serialised by the caller. src is ignored for
-   I2_CC. `iterations` may be NULL. */
+   stream); the call is synchronous: it waits for `stream` after every
+   iteration to read the frontier size, and returns when the result is in
+   dist_dev. The first call on each device looks up the scratch's device
+   address and keeps it for the life of the process; make that first call
+   before any stream capture, and make no call after a cudaDeviceReset of that
+   device. All calls share the one scratch: calls that overlap on the GPU
+   (other streams, other host threads) race and must be serialised by the
+   caller. Arrays on another GPU than the current one are refused
+   (I2_ERR_ARG), as are negative SSSP weights (I2_ERR_UNSUPPORTED, like
+   i2_sssp). src is ignored for I2_CC. `iterations` may be NULL. */
 int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* dist_dev, void* stream, int* iterations);
 
 /* ---- batches of graphs traversed together ---- */

@@ -149,6 +149,15 @@ __global__ void k_reset(Ctl* ctl, RunParams p) {
 // ---------------------------------------------------------------------------
 // Graph maintenance kernels.
 
+// Sets bit 8 of *bad when a weight is negative (SSSP needs weights >= 0).
+__global__ void k_negative_weights(const int* w, long long n, int* bad) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int neg = 0;
+  for (long long e = tid; e < n; e += stride) neg |= w[e] < 0;
+  if (__any_sync(0xffffffffu, neg) && (threadIdx.x & 31) == 0) atomicOr(bad, 8);
+}
+
 __global__ void k_validate(DGraph g, int* bad) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -1283,7 +1292,9 @@ int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
 
 // True when [p, p + bytes) lies inside one device (or managed) allocation of
 // the current context. Host pointers, pinned or not, are refused: a kernel
-// given one would fault or read the wrong memory.
+// given one would fault or read the wrong memory. So is device memory of
+// another GPU: kernels launched on the current device would read it through a
+// peer mapping, or fault where there is none.
 typedef int (*MemGetAddressRangeFn)(unsigned long long*, size_t*, unsigned long long);
 
 static bool device_range_ok(const void* p, size_t bytes) {
@@ -1295,6 +1306,13 @@ static bool device_range_ok(const void* p, size_t bytes) {
     return false;
   }
   if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+  if (a.type == cudaMemoryTypeDevice) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || a.device != cur) {
+      cudaGetLastError();
+      return false;
+    }
+  }
   static MemGetAddressRangeFn range_fn = nullptr;
   static bool looked = false;
   if (!looked) {
@@ -1649,9 +1667,12 @@ extern "C" int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* di
   int hbad = 0;
   I2_CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
   k_validate<<<4 * sm_count(), 256, 0, s>>>(c.g, bad);
+  // negative weights: refused like the allocating entry points refuse them
+  if (w) k_negative_weights<<<4 * sm_count(), 256, 0, s>>>(w, dev->edges, bad);
   I2_CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
   I2_CK(cudaStreamSynchronize(s));
-  if (hbad) return I2_ERR_FORMAT;
+  if (hbad & 7) return I2_ERR_FORMAT;
+  if (hbad & 8) return I2_ERR_UNSUPPORTED;
 
   // The scratch keeps the previous call's contents: the bitmaps must start at
   // zero (k_reset rewrites the control block, k_fill the output).

@@ -20,7 +20,6 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
-REFERENCE_ROOT = Path("/root/reference")
 
 _lib = None
 
@@ -49,6 +48,11 @@ def lib() -> C.CDLL:
         _lib.oracle_mis_priority.argtypes = [C.c_int]
         _lib.oracle_synth_weights.restype = None
         _lib.oracle_sp.restype = None
+        PP = C.POINTER(P)
+        _lib.oracle_gen_rmat.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                         C.c_int, P, P, PP, PP, PP]
+        _lib.oracle_graph_free.argtypes = [P, P, P]
+        _lib.oracle_graph_free.restype = None
     return _lib
 
 
@@ -59,6 +63,38 @@ def _p(a: np.ndarray):
 
 def _csr(g):
     return np.ascontiguousarray(g.nindex, np.int32), np.ascontiguousarray(g.nlist, np.int32)
+
+
+class Graph:
+    """A host CSR in the ECLgraph layout (nodes, edges, nindex, nlist, eweight)."""
+
+    def __init__(self, nodes: int, edges: int, nindex: np.ndarray, nlist: np.ndarray, eweight):
+        self.nodes, self.edges = nodes, edges
+        self.nindex, self.nlist, self.eweight = nindex, nlist, eweight
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.nindex)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1, weighted: bool = True) -> Graph:
+    """The seeded RMAT graph of graphgen.c (the same CSR as the engine's host
+    and device RMAT generators, built without the engine library)."""
+    P = C.POINTER(C.c_int)
+    n, e = C.c_int(), C.c_int()
+    ni, nl, ew = P(), P(), P()
+    rc = lib().oracle_gen_rmat(scale, edge_factor, a, b, c, seed, int(weighted), C.byref(n), C.byref(e),
+                               C.byref(ni), C.byref(nl), C.byref(ew))
+    if rc != 0:
+        raise ValueError(f"oracle_gen_rmat failed ({rc})")
+    try:
+        nindex = np.ctypeslib.as_array(ni, (n.value + 1,)).copy()
+        nlist = np.ctypeslib.as_array(nl, (e.value,)).copy() if e.value else np.zeros(0, np.int32)
+        eweight = (np.ctypeslib.as_array(ew, (e.value,)).copy() if e.value else np.zeros(0, np.int32)) \
+            if weighted else None
+    finally:
+        lib().oracle_graph_free(ni, nl, ew)
+    return Graph(n.value, e.value, nindex, nlist, eweight)
 
 
 def bfs(g, src: int) -> np.ndarray:

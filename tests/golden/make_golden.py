@@ -30,7 +30,8 @@ sys.path.insert(0, str(ROOT))
 import indigo2suite_b200 as i2  # noqa: E402
 import oracle  # noqa: E402
 
-SMALL = Path("/root/reference/small-inputs")
+# the reference tree: $I2_REFERENCE_ROOT (the same variable oracle/Makefile reads)
+SMALL = Path(os.environ.get("I2_REFERENCE_ROOT", "/root/reference")) / "small-inputs"
 
 
 def add_case(out: dict, name: str, g: i2.ECLGraph, sources: list[int]) -> None:

@@ -13,10 +13,21 @@ import oracle
 ROOT = Path(__file__).resolve().parents[1]
 
 
+# Runs bench.py's main() in this interpreter, then reports on stderr whether
+# the engine package or its library was ever loaded into the process.
+_PROBE = """
+import runpy, sys
+sys.argv = ["bench.py"] + sys.argv[1:]
+runpy.run_path("bench.py", run_name="__main__")
+maps = open("/proc/self/maps").read()
+sys.stderr.write("ENGINE_LOADED=%d\\n" % ("libi2b200" in maps or "indigo2suite_b200" in sys.modules))
+"""
+
+
 def _bench(env_extra, *args):
     env = dict(os.environ)
     env.update(env_extra)
-    return subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", *args],
+    return subprocess.run([sys.executable, "-c", _PROBE, "--impl", "reference", *args],
                           cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
 
 
@@ -39,3 +50,16 @@ def test_reference_arm_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "sssp_rmat22_ef16_edge_data_push"
+    # the reference arm runs no engine code, not even to build its input
+    assert "ENGINE_LOADED=0" in r.stderr
+    # and reports the config the GPU arm reports for the same graph
+    import argparse
+
+    import indigo2suite_b200 as i2
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    g = i2.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
+    args = argparse.Namespace(variant="vp_cta", loop="graph", delta=0)
+    assert d["config"] == bench.bench_config(args, g, 1)

@@ -174,3 +174,18 @@ def test_trim_without_device_is_a_status():
     with pytest.raises(i2.I2Error) as e:
         i2.trim_device_memory()
     assert e.value.status == _capi.I2_ERR_NO_DEVICE
+
+
+def test_noalloc_argument_checks_come_before_any_device_work():
+    """i2_run_noalloc refuses bad arguments with a status before it touches a
+    device (so these hold on a machine without one)."""
+    P = C.POINTER(C.c_int)
+    out = C.c_void_p(0x1000)
+    g = _capi.EclGraphC(10, 0, C.cast(C.c_void_p(0x1000), P), P(), P())
+    assert i2.lib.i2_run_noalloc(i2.I2_BFS, None, 0, out, None, None) == _capi.I2_ERR_ARG
+    assert i2.lib.i2_run_noalloc(i2.I2_BFS, C.byref(g), 0, None, None, None) == _capi.I2_ERR_ARG
+    assert i2.lib.i2_run_noalloc(7, C.byref(g), 0, out, None, None) == _capi.I2_ERR_ARG
+    assert i2.lib.i2_run_noalloc(i2.I2_BFS, C.byref(g), 10, out, None, None) == _capi.I2_ERR_ARG
+    assert i2.lib.i2_run_noalloc(i2.I2_SSSP, C.byref(g), 0, out, None, None) == _capi.I2_ERR_ARG  # no weights
+    big = _capi.EclGraphC((1 << 17) + 1, 0, C.cast(C.c_void_p(0x1000), P), P(), P())
+    assert i2.lib.i2_run_noalloc(i2.I2_BFS, C.byref(big), 0, out, None, None) == _capi.I2_ERR_CAPACITY

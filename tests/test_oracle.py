@@ -158,3 +158,17 @@ def test_mis_oracle_matches_reference_cpu_program():
         _, ref = oracle.ref_cpu_run("mis_cpp", g, 0, 4)
         np.testing.assert_array_equal(oracle.mis(g, unsigned_priority=True), ref)
     assert not np.array_equal(oracle.mis(g, unsigned_priority=False), ref)  # the two orders differ
+
+
+def test_oracle_rmat_generator_equals_engine_generator():
+    """oracle.gen_rmat (oracle/graphgen.c) restates the engine's seeded RMAT
+    graph independently; the benchmark's reference arm builds its input with it."""
+    for scale, seed in ((8, 3), (12, 22), (16, 5)):
+        a = oracle.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=seed)
+        b = i2.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=seed)
+        assert (a.nodes, a.edges) == (b.nodes, b.edges)
+        assert np.array_equal(a.nindex, b.nindex)
+        assert np.array_equal(a.nlist, b.nlist)
+        assert np.array_equal(a.eweight, b.eweight)
+    u = oracle.gen_rmat(10, 8, seed=1, weighted=False)
+    assert u.eweight is None and u.edges == i2.gen_rmat(10, 8, seed=1, weighted=False).edges
