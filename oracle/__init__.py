@@ -53,6 +53,8 @@ def lib() -> C.CDLL:
                                          C.c_int, P, P, PP, PP, PP]
         _lib.oracle_graph_free.argtypes = [P, P, P]
         _lib.oracle_graph_free.restype = None
+        _lib.oracle_certify_distances.argtypes = [C.c_int, P, P, P, C.c_int, P]
+        _lib.oracle_certify_cc.argtypes = [C.c_int, P, P, P]
     return _lib
 
 
@@ -249,60 +251,36 @@ def run_ref_program(name: str, args: list[str], threads: int | None = None, time
 
 
 # ---------------------------------------------------------------------------
-# Size-independent certificates (vectorised numpy), for sizes where running
-# the serial oracle is too slow.
+# Size-independent certificates (certify.c, parallel C), for sizes where
+# running the serial oracle is too slow.
+
+_DIST_FAIL = {1: "dist[src] != 0", 2: "negative value", 3: "unreached neighbour of a reached vertex",
+              4: "relaxable edge", 5: "reached vertex without a tight in-edge", 6: "weight below 1",
+              -1: "out of memory", -2: "bad arguments"}
+_CC_FAIL = {1: "adjacent labels differ", 2: "label above its vertex id", 3: "label is not its own label",
+            4: "vertex not connected to its label", -1: "out of memory", -2: "bad arguments"}
+
 
 def certify_distances(g, src: int, dist: np.ndarray, weighted: bool) -> str | None:
-    """Shortest-path certificate: dist[src] == 0; dist[v] <= dist[u] + w(u, v) on
-    every edge; every other reached vertex has a tight in-edge; unreached
-    vertices have no reached neighbour. Returns None when it holds."""
-    INF = np.iinfo(np.int32).max
-    d = np.asarray(dist, np.int64)
-    if d[src] != 0:
-        return "dist[src] != 0"
-    deg = np.diff(np.asarray(g.nindex, np.int64))
-    u = np.repeat(np.arange(g.nodes, dtype=np.int64), deg)
-    v = np.asarray(g.nlist, np.int64)
-    w = np.asarray(g.eweight, np.int64) if weighted else np.ones(g.edges, np.int64)
-    du, dv = d[u], d[v]
-    reached_u = du != INF
-    if (dv[reached_u] == INF).any():
-        return "unreached neighbour of a reached vertex"
-    cand = du + w
-    if (dv[reached_u] > cand[reached_u]).any():
-        return "relaxable edge"
-    tight = np.zeros(g.nodes, bool)
-    tv = v[reached_u & (dv == cand)]
-    tight[tv] = True
-    reached = d != INF
-    reached[src] = False
-    if not tight[reached].all():
-        return "reached vertex without a tight in-edge"
-    return None
+    """Shortest-path certificate (weights >= 1): dist[src] == 0; dist[v] <=
+    dist[u] + w(u, v) on every edge out of a reached vertex, whose neighbours
+    are all reached; every other reached vertex has a tight in-edge. Returns
+    None when it holds, else what failed."""
+    ni, nl = _csr(g)
+    w = _p(np.ascontiguousarray(g.eweight, np.int32)) if weighted else None
+    d = np.ascontiguousarray(dist, np.int32)
+    rc = lib().oracle_certify_distances(g.nodes, _p(ni), _p(nl), w, int(src), _p(d))
+    return None if rc == 0 else _DIST_FAIL.get(rc, f"code {rc}")
 
 
 def certify_cc(g, label: np.ndarray) -> str | None:
     """Minimum-label certificate on a symmetric graph: labels equal across every
-    edge, label[v] <= v, label[label[v]] == label[v], and as many distinct labels
-    as components (union-find in numpy by repeated min-propagation is avoided:
-    the count comes from scipy's connected_components)."""
-    from scipy.sparse import csr_matrix
-    from scipy.sparse.csgraph import connected_components
-
-    lab = np.asarray(label, np.int64)
-    deg = np.diff(np.asarray(g.nindex, np.int64))
-    u = np.repeat(np.arange(g.nodes, dtype=np.int64), deg)
-    if (lab[u] != lab[np.asarray(g.nlist, np.int64)]).any():
-        return "adjacent labels differ"
-    if (lab > np.arange(g.nodes)).any() or (lab < 0).any():
-        return "label above its vertex id"
-    if (lab[lab] != lab).any():
-        return "label is not its own label"
-    m = csr_matrix((np.ones(g.edges, np.int8), np.asarray(g.nlist), np.asarray(g.nindex)), shape=(g.nodes, g.nodes))
-    ncomp, _ = connected_components(m, directed=False)
-    if len(np.unique(lab)) != ncomp:
-        return "label count != component count"
-    return None
+    edge, 0 <= label[v] <= v, label[label[v]] == label[v], and every vertex
+    connected to the vertex its label names. Returns None when it holds."""
+    ni, nl = _csr(g)
+    lab = np.ascontiguousarray(label, np.int32)
+    rc = lib().oracle_certify_cc(g.nodes, _p(ni), _p(nl), _p(lab))
+    return None if rc == 0 else _CC_FAIL.get(rc, f"code {rc}")
 
 
 def certify_mis(g, status: np.ndarray) -> str | None:

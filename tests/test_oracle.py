@@ -172,3 +172,61 @@ def test_oracle_rmat_generator_equals_engine_generator():
         assert np.array_equal(a.eweight, b.eweight)
     u = oracle.gen_rmat(10, 8, seed=1, weighted=False)
     assert u.eweight is None and u.edges == i2.gen_rmat(10, 8, seed=1, weighted=False).edges
+
+
+def test_certificates_accept_oracle_results_and_catch_planted_mistakes():
+    """The size-independent certificates (oracle/certify.c) used at full size
+    accept the oracle's own answers and reject each kind of planted error."""
+    g = i2.gen_rmat(14, 16, seed=9)
+    src = int(np.argmax(g.degrees()))
+    d = oracle.sssp(g, src)
+    b = oracle.bfs(g, src)
+    assert oracle.certify_distances(g, src, d, weighted=True) is None
+    assert oracle.certify_distances(g, src, b, weighted=False) is None
+    assert oracle.certify_distances(g, src, d, weighted=False) is not None  # wrong metric
+    reached = np.flatnonzero((d != INF) & (np.arange(g.nodes) != src))
+    v = int(reached[len(reached) // 2])
+    bad = d.copy()
+    bad[v] += 1  # too large: an in-edge is relaxable
+    assert oracle.certify_distances(g, src, bad, weighted=True) == "relaxable edge"
+    bad = d.copy()
+    bad[v] -= 1  # too small: no tight in-edge
+    assert oracle.certify_distances(g, src, bad, weighted=True) == "reached vertex without a tight in-edge"
+    bad = d.copy()
+    bad[v] = INF
+    assert oracle.certify_distances(g, src, bad, weighted=True) == "unreached neighbour of a reached vertex"
+    bad = d.copy()
+    bad[src] = 1
+    assert oracle.certify_distances(g, src, bad, weighted=True) == "dist[src] != 0"
+    lab = oracle.cc(g)
+    assert oracle.certify_cc(g, lab) is None
+    bad = lab.copy()
+    u = int(np.flatnonzero(g.degrees() > 0)[-1])
+    bad[u] = u  # splits a component
+    assert oracle.certify_cc(g, bad) in ("adjacent labels differ", "label is not its own label")
+    # two components merged under one label: the labels are consistent across
+    # edges, but the second component is not connected to the label's root
+    comps = {}
+    for x in range(g.nodes):
+        comps.setdefault(int(lab[x]), []).append(x)
+    roots = sorted(r for r, m in comps.items() if len(m) > 1)
+    if len(roots) < 2:  # an extra edge pair component for the case
+        pytest.skip("graph has one non-trivial component")
+    r0, r1 = roots[0], roots[1]
+    bad = lab.copy()
+    bad[np.array(comps[r1])] = r0
+    assert oracle.certify_cc(g, bad) == "vertex not connected to its label"
+    bad = lab.copy()
+    bad[r1] = r1 + 1 if r1 + 1 < g.nodes else r1 - 1
+    assert oracle.certify_cc(g, bad) is not None
+
+
+def test_cc_certificate_on_a_graph_of_many_components():
+    g = i2.gen_grid(40, 0.45, 0.0, seed=11)  # many small components
+    lab = oracle.cc(g)
+    assert len(np.unique(lab)) > 10
+    assert oracle.certify_cc(g, lab) is None
+    comps = sorted(set(int(x) for x in lab))
+    bad = lab.copy()
+    bad[lab == comps[-1]] = comps[-2]
+    assert oracle.certify_cc(g, bad) == "vertex not connected to its label"
