@@ -466,6 +466,8 @@ def run_er16(args, rank: int, world: int, local: int):
     dg = i2.DeviceGraph.upload(g)
     ref = oracle.bfs(g, 0)
     res = {}
+    clocks = Clocks(local)
+    clocks.start()
     for v in ("vp_cta", "heuristic"):
         d, _ = dg.bfs(0, variant=v)
         if not np.array_equal(d, ref):
@@ -475,6 +477,7 @@ def run_er16(args, rank: int, world: int, local: int):
             run()
         torch.cuda.synchronize()
         res[v] = _event_time(torch, stream, run, args.steps)
+    clk = clocks.stop()
     dist.barrier()
     t = dist.max(res["vp_cta"], dev)
     cpu = {}
@@ -500,7 +503,7 @@ def run_er16(args, rank: int, world: int, local: int):
             "heuristic_gteps": world * 1e-9 * g.edges / dist.max(res["heuristic"], dev),
             "cpu_baseline": (dict(best, kind="reference", sample="full graph, median of 3 of the program's own timer",
                                   all=cpu) if best else None),
-            "verified": "bit-exact vs the oracle (GPU and reference CPU programs)"}
+            "clocks": clk, "verified": "bit-exact vs the oracle (GPU and reference CPU programs)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     dg.free()
@@ -610,10 +613,17 @@ def run_grid4096(args, rank: int, world: int, local: int):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
+    import oracle
+
     g = i2.gen_grid(4096, 0.05, 0.001, seed=3)
     dg = i2.DeviceGraph.upload(g)
     if SELECTOR_PARAMS.exists():
         i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
+    # every measured configuration's result, bit-exact against the oracle
+    refs = {i2.I2_BFS: oracle.bfs(g, 0), i2.I2_CC: oracle.cc(g)}
+    verified = {}
+    clocks = Clocks(local)
+    clocks.start()
     out = {}
     for an, algo in (("bfs", i2.I2_BFS), ("cc", i2.I2_CC)):
         res = {}
@@ -625,6 +635,10 @@ def run_grid4096(args, rank: int, world: int, local: int):
             run()
             torch.cuda.synchronize()
             res[name] = 1e3 * _event_time(torch, stream, run, max(1, args.steps // 5))
+            got = dg._run(algo, 0, v, i2.I2_LOOP_GRAPH, 0, False, None)[0]
+            if not np.array_equal(got, refs[algo]):
+                raise SystemExit(f"grid4096 {an} {name}: result differs from the oracle")
+            verified[f"{an}/{name}"] = "bit-exact vs oracle"
         rep = dg.run_device(algo, 0, variant="learned")
         fixed = {k: t for k, t in res.items() if k not in ("heuristic", "learned")}
         best = min(fixed, key=fixed.get)
@@ -636,7 +650,7 @@ def run_grid4096(args, rank: int, world: int, local: int):
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": "grid4096_bfs_cc_selector", "nodes": g.nodes, "edges": g.edges,
                        "remove": 0.05, "long_range": 0.001, "source": 0},
-            "results": out}
+            "results": out, "clocks": clocks.stop(), "verified": verified}
     print(json.dumps(line), flush=True)
     dg.free()
 
@@ -670,6 +684,8 @@ def run_rmat26(args, rank: int, world: int, local: int):
     mine = srcs[lo:hi]
     res = {}
     peak, peak_kind = peaks()
+    clocks = Clocks(local)
+    clocks.start()
     for an, algo in (("bfs", i2.I2_BFS), ("sssp", i2.I2_SSSP), ("cc", i2.I2_CC)):
         # algorithmic bytes per traversal (reached counts of the first source:
         # every source with an edge lies in the giant component)
@@ -688,13 +704,35 @@ def run_rmat26(args, rank: int, world: int, local: int):
             res[f"{an}/{v}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t,
                                 "b_alg_gb": 1e-9 * b_alg, "achieved_gbs": 1e-9 * b_alg / t,
                                 "roofline_frac": 1e-9 * b_alg / t / peak}
+    clk = clocks.stop()
+    # results of the measured configurations from two of this rank's sources,
+    # checked by the size-independent certificates (no serial run over 2e9 edges)
+    import oracle
+
+    host = dg.download()
+    verified = {}
+    for s_ in mine[:2]:
+        for v in ("vp_cta", "heuristic", "learned"):
+            for an, algo, wt in (("bfs", i2.I2_BFS, False), ("sssp", i2.I2_SSSP, True)):
+                d = dg._run(algo, s_, v, i2.I2_LOOP_GRAPH, 0, False, None)[0]
+                c = oracle.certify_distances(host, s_, d, weighted=wt)
+                if c is not None:
+                    raise SystemExit(f"rmat26 {an} {v} source {s_}: certificate failed: {c}")
+                verified[f"{an}/{v}/src{s_}"] = "shortest-path certificate"
+    for v in ("vp_cta", "heuristic", "learned"):
+        lab = dg._run(i2.I2_CC, 0, v, i2.I2_LOOP_GRAPH, 0, False, None)[0]
+        c = oracle.certify_cc(host, lab)
+        if c is not None:
+            raise SystemExit(f"rmat26 cc {v}: certificate failed: {c}")
+        verified[f"cc/{v}"] = "minimum-label certificate"
+    del host
     line = {"metric": METRIC, "value": world * res["bfs/learned"]["gteps"], "unit": UNIT, "n_gpus": world,
             "steps": 64, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": "rmat26_bfs_sssp_cc_64src", "nodes": dg.nodes, "edges": dg.edges,
                        "generation_s": gen_s, "parallelism": f"sources sharded x{world}"},
             "roofline_peak_gbs": peak, "roofline_peak_source": peak_kind,
-            "results": res}
+            "results": res, "clocks": clk, "verified": verified}
     if rank == 0:
         print(json.dumps(line), flush=True)
     dg.free()
