@@ -6,9 +6,11 @@ edge factor 16, a=0.57 b=0.19 c=0.19 d=0.05, seed 22), symmetrised,
 deduplicated, no self-loops, int32 weights uniform in [1,255] (one per
 undirected edge), source = highest-degree vertex (lowest ID on ties); fixed
 style: edge-centric data-driven push (the engine's vp_cta: one thread per
-frontier edge). A step is one complete SSSP traversal (init + all iterations)
-with the graph resident in HBM; nlist + eweight (1 GB) exceed L2, so every step
-streams them from HBM.
+frontier edge), with the budgeted near/far ordering (each iteration relaxes
+the frontier vertices below a distance threshold that keeps about 4.2M edges
+below it; --budget 0 turns it off). A step is one complete SSSP traversal
+(init + all iterations) with the graph resident in HBM; nlist + eweight (1 GB)
+exceed L2, so every step streams them from HBM.
 
 value   : GTEPS, reference definition (1e-9 * g.edges / seconds per traversal,
           include/bfs_vertex_cuda.h:163), summed over all ranks.
@@ -50,7 +52,9 @@ KERNEL_NAMES = {"vp_thread": "relax_push", "vp_warp": "relax_push", "vp_cta": "r
                 "edge_topo": "relax_edge_topo", "push_topo": "relax_push_topo"}
 WORKLOAD = {"workload": "sssp_rmat22_ef16_edge_data_push", "graph": "rmat", "scale": 22, "edge_factor": 16,
             "a": 0.57, "b": 0.19, "c": 0.19, "seed": 22, "weights": "uniform[1,255]",
-            "source": "highest-degree vertex", "algorithm": "sssp", "style": "vp_cta (edge-centric data-driven push)",
+            "source": "highest-degree vertex", "algorithm": "sssp",
+            "style": "vp_cta (edge-centric data-driven push; vertices relaxed in distance order by the budgeted "
+                     "near/far ordering unless near_far_budget is off)",
             "l2": "inputs larger than L2 (nlist+eweight 1.0 GB)"}
 SELECTOR_PARAMS = ROOT / "indigo2suite_b200" / "selector_params.bin"
 
@@ -220,7 +224,9 @@ def bench_config(args, g, world: int) -> dict:
     """The benchmark line's `config`, identical in both arms."""
     return dict(WORKLOAD, variant=args.variant, edges=g.edges, nodes=g.nodes, graph_sha16=graph_digest(g),
                 parallelism=f"replicas x{world}", loop=args.loop,
-                near_far_step=args.delta if args.delta > 0 else "off")
+                near_far_step=args.delta if args.delta > 0 else "off",
+                near_far_budget=("off" if args.delta > 0 or args.budget == 0 else
+                                 "auto (28672 edges per SM)" if args.budget < 0 else args.budget))
 
 
 def run_reference(args, rank: int, world: int):
@@ -277,7 +283,8 @@ def run_ours(args, rank: int, world: int, local: int):
 
     # correctness of the measured configuration (shortest-path certificate)
     delta = args.delta
-    d, rep = dg.sssp(src, variant=variant, delta=delta)
+    budget = -1 if args.budget < 0 else args.budget  # I2_SSSP_BUDGET_AUTO when negative
+    d, rep = dg.sssp(src, variant=variant, delta=delta, budget=budget)
     import oracle
 
     cert = oracle.certify_distances(host, src, d, weighted=True)
@@ -286,10 +293,10 @@ def run_ours(args, rank: int, world: int, local: int):
 
     loop = {"graph": i2.I2_LOOP_GRAPH, "host": i2.I2_LOOP_HOST, "relaunch": i2.I2_LOOP_RELAUNCH}[args.loop]
 
-    def steps(n, v=variant):
+    def steps(n, v=variant, b=None):
         for _ in range(n):
             dg.run_device(i2.I2_SSSP, src, variant=v, stream=sp, loop=loop, report=loop == i2.I2_LOOP_HOST,
-                          delta=delta)
+                          delta=delta, budget=budget if b is None else b)
 
     with torch.cuda.stream(stream):
         steps(args.warmup)
@@ -317,8 +324,9 @@ def run_ours(args, rank: int, world: int, local: int):
     # before it are < 2% of the step and are charged to it). The host-driven
     # loop's per-iteration launches, each bracketed by CUDA events, are
     # reported beside it.
-    rep_h = dg.run_device(i2.I2_SSSP, src, variant=variant, loop=i2.I2_LOOP_HOST, stream=sp, delta=delta)
-    rep_g = dg.run_device(i2.I2_SSSP, src, variant=variant, stream=sp, delta=delta)
+    rep_h = dg.run_device(i2.I2_SSSP, src, variant=variant, loop=i2.I2_LOOP_HOST, stream=sp, delta=delta,
+                          budget=budget)
+    rep_g = dg.run_device(i2.I2_SSSP, src, variant=variant, stream=sp, delta=delta, budget=budget)
     b_alg = 12.0 * rep_g.reached_edges + 20.0 * rep_g.reached_vertices
     graph_loop = loop == i2.I2_LOOP_GRAPH
     kernel_s = ms_max * 1e-3 if graph_loop else rep_h.relax_seconds
@@ -343,7 +351,7 @@ def run_ours(args, rank: int, world: int, local: int):
 
     # the other styles and the selectors (a few steps each)
     styles = {}
-    cand = list(range(i2.I2_NUM_VARIANTS)) + ["heuristic"]
+    cand = list(range(i2.I2_NUM_VARIANTS)) + ["vp_cta_plain", "heuristic"]
     if SELECTOR_PARAMS.exists():
         i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
         cand.append("learned")
@@ -353,12 +361,15 @@ def run_ours(args, rank: int, world: int, local: int):
             continue
         if v == 8:  # union-find computes CC labels only
             continue
+        b = None
+        if v == "vp_cta_plain":  # the edge-balanced push without the near/far ordering
+            v, b = "vp_cta", 0
         with torch.cuda.stream(stream):
-            steps(1, v)
+            steps(1, v, b)
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(stream)
-        steps(args.style_steps, v)
+        steps(args.style_steps, v, b)
         f1.record(stream)
         f1.synchronize()
         styles[name] = 1e-9 * E / (f0.elapsed_time(f1) / args.style_steps * 1e-3)
@@ -375,7 +386,7 @@ def run_ours(args, rank: int, world: int, local: int):
         t0 = time.perf_counter()
         gg = i2.DeviceGraph.upload(hp)
         t1 = time.perf_counter()
-        gg.sssp(src, variant=variant, out=out, delta=delta)
+        gg.sssp(src, variant=variant, out=out, delta=delta, budget=budget)
         t2 = time.perf_counter()
         gg.free()
         torch.cuda.synchronize()
@@ -391,7 +402,7 @@ def run_ours(args, rank: int, world: int, local: int):
            "query_only_note": "per-query C-ABI call on a resident graph: see e2e_query"}
     q0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        dg.sssp(src, variant=variant, out=out, delta=delta)
+        dg.sssp(src, variant=variant, out=out, delta=delta, budget=budget)
     q_s = (time.perf_counter() - q0) / args.e2e_steps
     e2e_query = {"value": world * 1e-9 * E / dist.max(q_s, dev), "unit": UNIT, "h2d_bytes_per_step": 4,
                  "d2h_bytes_per_step": 4 * V}
@@ -444,6 +455,43 @@ def _event_time(torch, stream, fn, steps: int) -> float:
     return e0.elapsed_time(e1) * 1e-3 / steps
 
 
+def er16_cpu_programs(g) -> dict:
+    """Every reference OpenMP (38) and C++-threads (40) BFS program, built
+    unchanged, on the ER graph from vertex 0 through its own main(): the
+    median of its 3 runs and its own verifier's verdict, at all host threads
+    and at one. Best and median over the programs whose verifier passed."""
+    import oracle
+
+    progs = oracle.bfs_programs()
+    if not progs:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "unavailable: oracle/_ref/bfs_{omp,cpp} not built"}
+    nproc = os.cpu_count() or 1
+    runs = {}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "er16.egr")
+        oracle.write_egr(g, path)
+        for th in (nproc, 1):
+            for model, name in progs:
+                r = oracle.run_bfs_program(model, name, path, 0, th)
+                runs.setdefault(str(th), {})[f"{model}/{name}"] = {
+                    "gteps": 1e-9 * g.edges / r["runtime"] if r["runtime"] else None,
+                    "seconds": r["runtime"], "verified": r["verified"] and r["rc"] == 0}
+    summary = {}
+    for th, rs in runs.items():
+        ok = {k: v["gteps"] for k, v in rs.items() if v["verified"] and v["gteps"]}
+        best = max(ok, key=ok.get) if ok else None
+        summary[th] = {"programs": len(rs), "verified": len(ok),
+                       "failed_own_verifier": sorted(k for k, v in rs.items() if not v["verified"]),
+                       "best": {"program": best, "gteps": ok[best]} if best else None,
+                       "median_gteps": statistics.median(ok.values()) if ok else None}
+    top = summary[str(nproc)]["best"]
+    return {"value": top["gteps"] if top else None, "unit": UNIT, "cores": nproc, "kind": "reference",
+            "program": top["program"] if top else None,
+            "sample": "full graph; each program's own main(): median of its 3 runs, its own verifier",
+            "summary": summary, "all": runs}
+
+
 def run_er16(args, rank: int, world: int, local: int):
     """Config: ER G(n=65,536, m=262,144 distinct undirected pairs) = 524,288 CSR
     entries, BFS from vertex 0 -- the reference's CPU configuration. Our GPU
@@ -480,20 +528,9 @@ def run_er16(args, rank: int, world: int, local: int):
     clk = clocks.stop()
     dist.barrier()
     t = dist.max(res["vp_cta"], dev)
-    cpu = {}
+    cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        nproc = os.cpu_count() or 1
-        for prog in ("bfs_omp", "bfs_cpp"):
-            for th in (nproc, 1):
-                ts = []
-                for _ in range(3):
-                    tt, out = oracle.ref_cpu_run(prog, g, 0, th)
-                    ts.append(tt)
-                if not np.array_equal(out, ref):
-                    raise SystemExit(f"reference {prog} result differs from the oracle")
-                cpu[f"{prog}_{th}t"] = {"value": 1e-9 * g.edges / statistics.median(ts), "unit": UNIT,
-                                        "cores": th, "seconds": statistics.median(ts)}
-    best = max(cpu.values(), key=lambda x: x["value"]) if cpu else None
+        cpu = er16_cpu_programs(g)
     line = {"metric": METRIC, "value": world * 1e-9 * g.edges / t, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
@@ -501,8 +538,7 @@ def run_er16(args, rank: int, world: int, local: int):
                        "variant": "vp_cta", "l2": "graph fits in L2 (2.4 MB): launch-latency bound",
                        "parallelism": f"replicas x{world}"},
             "heuristic_gteps": world * 1e-9 * g.edges / dist.max(res["heuristic"], dev),
-            "cpu_baseline": (dict(best, kind="reference", sample="full graph, median of 3 of the program's own timer",
-                                  all=cpu) if best else None),
+            "cpu_baseline": cpu,
             "clocks": clk, "verified": "bit-exact vs the oracle (GPU and reference CPU programs)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -746,6 +782,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--variant", default="vp_cta")
+    ap.add_argument("--budget", type=int, default=-1,
+                    help="SSSP budgeted near/far ordering of the vp_cta style: < 0 the engine's default "
+                         "budget (28672 edges per SM), 0 off, > 0 edges per near set")
     ap.add_argument("--delta", type=int, default=0,
                     help="SSSP near/far threshold step of the vp_cta style: <= 0 off, > 0 this step")
     ap.add_argument("--style-steps", type=int, default=3)

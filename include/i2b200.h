@@ -97,7 +97,18 @@ typedef struct {
                        from iteration then_at on (a fixed switch of style; results do
                        not change). 0: no switch. */
   int then_variant;
+  int sssp_budget;  /* SSSP with I2_VP_CTA only, when sssp_delta <= 0: budgeted
+                       near/far ordering. Each iteration relaxes only the frontier
+                       vertices below a distance threshold that the engine sets on
+                       the device so that about `sssp_budget` edges lie below it
+                       (from distance histograms of the frontier, and of the far
+                       pile when the frontier runs dry); the rest wait on the far
+                       pile. 0: off; > 0: this many edges;
+                       I2_SSSP_BUDGET_AUTO: the engine's default (28672 per SM).
+                       The distances do not depend on it. */
 } i2_opts;
+
+#define I2_SSSP_BUDGET_AUTO (-1)
 
 typedef struct {
   double seconds;          /* device time of init + all iterations (CUDA events) */
@@ -120,6 +131,11 @@ typedef struct {
   long long visited;       /* vertices reached before this launch */
   unsigned long long t_ns; /* launch duration (device timer) */
   float feat[16];          /* selector features of the consumed frontier */
+  int kind;                /* SSSP near/far ordering: 0 relaxation, 1 move from the far pile,
+                              3 frontier trim (nothing is relaxed in 1 and 3) */
+  int threshold;           /* near/far threshold the launch used (INT_MAX: none) */
+  unsigned pile;           /* far-pile entries after the launch (live or superseded) */
+  int pad;
 } i2_iter_record;
 
 typedef struct {

@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi as capi
-from ._capi import (I2_AUTO_HEURISTIC, I2_AUTO_LEARNED, I2_BFS, I2_CC, I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH,
+from ._capi import (I2_SSSP_BUDGET_AUTO, I2_AUTO_HEURISTIC, I2_AUTO_LEARNED, I2_BFS, I2_CC, I2_LOOP_GRAPH, I2_LOOP_HOST, I2_LOOP_RELAUNCH,
                     I2_MIS, MIS_IN, MIS_OUT,
                     I2_NUM_VARIANTS, I2_SSSP, VARIANTS)
 
@@ -36,7 +36,7 @@ __all__ = [
     "GPUsssp_vertex", "GPUsssp_edge", "GPUcc_vertex", "GPUcc_edge", "mlp_param_count", "mlp_loss_grad",
     "mlp_train", "mlp_predict", "mlp_set_params", "device_count", "I2_BFS", "I2_SSSP", "I2_CC", "I2_MIS",
     "MIS_IN", "MIS_OUT", "GPUmis_vertex", "GPUmis_edge", "mis_priority",
-    "I2_AUTO_HEURISTIC", "I2_AUTO_LEARNED", "I2_NUM_VARIANTS", "I2_LOOP_GRAPH", "I2_LOOP_HOST", "I2_LOOP_RELAUNCH",
+    "I2_AUTO_HEURISTIC", "I2_AUTO_LEARNED", "I2_SSSP_BUDGET_AUTO", "I2_NUM_VARIANTS", "I2_LOOP_GRAPH", "I2_LOOP_HOST", "I2_LOOP_RELAUNCH",
 ]
 
 INF = np.iinfo(np.int32).max
@@ -183,13 +183,16 @@ class Report:
     status: int = 0
 
 
-def _opts(variant, loop, iter_cap, record, stream, delta: int = 0, then_variant=None, then_at: int = 0) -> capi.Opts:
+def _opts(variant, loop, iter_cap, record, stream, delta: int = 0, then_variant=None, then_at: int = 0,
+          budget: int = 0) -> capi.Opts:
     """delta: SSSP near/far threshold step for the vp_cta style (<= 0 off, > 0 this step).
+    budget: SSSP budgeted near/far ordering for the vp_cta style when delta <= 0 (0 off,
+    > 0 frontier edges per near set, I2_SSSP_BUDGET_AUTO the engine's default).
     then_variant/then_at: switch to then_variant from iteration then_at on."""
     tv = variant_id(then_variant) if then_variant is not None else 0
     return capi.Opts(variant_id(variant), int(loop), int(iter_cap), int(record),
                      C.c_void_p(stream) if stream else None, int(delta), int(then_at) if then_variant is not None else 0,
-                     tv)
+                     tv, int(budget))
 
 
 def _report(r: capi.Report, status: int) -> Report:
@@ -269,10 +272,10 @@ class DeviceGraph:
 
     # -- traversals ---------------------------------------------------------
     def _run(self, algo: int, src: int, variant, loop, iter_cap, record, stream, out=None, delta=0,
-             then_variant=None, then_at=0):
+             then_variant=None, then_at=0, budget=0):
         dist = out if out is not None else np.empty(self.nodes, np.int32)
         assert dist.dtype == np.int32 and dist.size >= self.nodes and dist.flags.c_contiguous
-        o = _opts(variant, loop, iter_cap, record, stream, delta, then_variant, then_at)
+        o = _opts(variant, loop, iter_cap, record, stream, delta, then_variant, then_at, budget)
         r = capi.Report()
         if algo == I2_BFS:
             st = lib.i2_bfs(self._h, src, _iptr(dist), C.byref(o), C.byref(r))
@@ -291,8 +294,9 @@ class DeviceGraph:
         return self._run(I2_BFS, src, variant, loop, iter_cap, record, stream, out, 0, then_variant, then_at)
 
     def sssp(self, src: int, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
-             delta: int = 0, then_variant=None, then_at: int = 0):
-        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out, delta, then_variant, then_at)
+             delta: int = 0, then_variant=None, then_at: int = 0, budget: int = 0):
+        return self._run(I2_SSSP, src, variant, loop, iter_cap, record, stream, out, delta, then_variant, then_at,
+                         budget)
 
     def cc(self, variant="vp_cta", loop=I2_LOOP_GRAPH, iter_cap=0, record=False, stream=None, out=None,
            then_variant=None, then_at: int = 0):
@@ -303,10 +307,11 @@ class DeviceGraph:
         return self._run(I2_MIS, 0, "vp_warp", loop, iter_cap, record, stream, out)
 
     def run_device(self, algo: int, src: int = 0, out_ptr: int = 0, variant="vp_cta", loop=I2_LOOP_GRAPH,
-                   iter_cap=0, record=False, stream=None, report: bool = True, delta: int = 0) -> Report | None:
+                   iter_cap=0, record=False, stream=None, report: bool = True, delta: int = 0,
+                   budget: int = 0) -> Report | None:
         """Traversal with the result left in device memory (copied to out_ptr if given).
         With report=False and the graph loop the call is asynchronous on `stream`."""
-        o = _opts(variant, loop, iter_cap, record, stream, delta)
+        o = _opts(variant, loop, iter_cap, record, stream, delta, budget=budget)
         r = capi.Report()
         st = lib.i2_run_device(self._h, algo, src, C.c_void_p(out_ptr) if out_ptr else None, C.byref(o),
                                C.byref(r) if report else None)
@@ -332,7 +337,8 @@ class DeviceGraph:
 
 def _rec(r: capi.IterRecord) -> dict:
     return {"iter": r.iter, "variant": r.variant, "size": r.size, "hsize": r.hsize, "edges": r.edges,
-            "maxdeg": r.maxdeg, "mindist": r.mindist, "visited": r.visited, "t_ns": r.t_ns,
+            "maxdeg": r.maxdeg, "mindist": r.mindist, "visited": r.visited, "t_ns": r.t_ns, "kind": r.kind,
+            "threshold": r.threshold, "pile": r.pile,
             "feat": np.array(list(r.feat), np.float32)}
 
 

@@ -31,6 +31,7 @@ MIS_IN, MIS_OUT = 1, 2  # status values of i2_mis (the reference's included / ex
 
 I2_AUTO_HEURISTIC = -1
 I2_AUTO_LEARNED = -2
+I2_SSSP_BUDGET_AUTO = -1
 VARIANTS = ["vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo", "edge_topo", "push_topo",
             "union_find"]
 I2_NUM_VARIANTS = len(VARIANTS)
@@ -47,7 +48,7 @@ class EclGraphC(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("variant", C.c_int), ("loop_mode", C.c_int), ("iter_cap", C.c_int),
                 ("record_iters", C.c_int), ("stream", C.c_void_p), ("sssp_delta", C.c_int),
-                ("then_at", C.c_int), ("then_variant", C.c_int)]
+                ("then_at", C.c_int), ("then_variant", C.c_int), ("sssp_budget", C.c_int)]
 
 
 class Report(C.Structure):
@@ -59,7 +60,8 @@ class Report(C.Structure):
 class IterRecord(C.Structure):
     _fields_ = [("iter", C.c_int), ("variant", C.c_int), ("size", C.c_int), ("hsize", C.c_int),
                 ("edges", C.c_ulonglong), ("maxdeg", C.c_int), ("mindist", C.c_int),
-                ("visited", C.c_longlong), ("t_ns", C.c_ulonglong), ("feat", C.c_float * NUM_FEATURES)]
+                ("visited", C.c_longlong), ("t_ns", C.c_ulonglong), ("feat", C.c_float * NUM_FEATURES),
+                ("kind", C.c_int), ("threshold", C.c_int), ("pile", C.c_uint), ("pad", C.c_int)]
 
 
 class GraphInfo(C.Structure):

@@ -21,7 +21,7 @@
 //   the current dist[]. Iteration i propagates at least F_i and builds F_{i+1}
 //   in slot (i+1) % 3 from every vertex whose value it lowered. It also clears
 //   slot (i+2) % 3 (F_{i-1}), which no variant reads during iteration i.
-// SSSP near/far ordering (Ctl::delta > 0) relaxes the contract in one way: a
+// SSSP near/far ordering (Ctl::delta != 0) relaxes the contract in one way: a
 // lowered vertex whose new distance is at or above the current threshold goes
 // onto the far pile instead of F_{i+1}. The traversal ends when both F_{i+1}
 // and the pile are empty. Only the edge-balanced push defers; every other
@@ -42,6 +42,7 @@ constexpr int kHeavyTile = 2048;     // edges per tile of a heavy vertex
 constexpr int kMaxVariants = 16;
 constexpr int kFeatures = 16;        // selector input width
 constexpr int kHidden = 64;          // selector hidden width (two layers)
+constexpr int kHistBins = 256;       // distance histogram of the budgeted near/far ordering
 
 enum Algo { kBFS = 0, kSSSP = 1, kCC = 2, kMIS = 3 };
 
@@ -141,16 +142,28 @@ struct Ctl {
   int sel_n;                // frontier entries at the last selector evaluation
   unsigned sel_e;           // frontier edges at the last selector evaluation
   int sel_iter;             // iteration of the last selector evaluation
-  // SSSP near/far ordering (delta > 0 only): relax iterations push values at
+  // SSSP near/far ordering (delta != 0 only): relax iterations push values at
   // or above `threshold` onto far pile `pcur` instead of the next frontier;
   // when the next frontier is empty and the pile is not, the next launch is a
-  // split (split = 1): the threshold rises to max(threshold, pmin) + delta and
-  // the pile's entries below it move into the next frontier, the others onto
-  // the other pile.
+  // split (split = 1): the threshold rises and the pile's entries below it
+  // move into the next frontier, the others onto the other pile.
+  //  * delta > 0 (fixed step): the threshold rises to max(threshold, pmin) + delta.
+  //  * delta < 0 (edge budget B = -delta): the threshold is set so that about
+  //    B edges lie below it, from distance histograms (weighted by degree)
+  //    that the launches keep of the next frontier and of the pile: a move
+  //    takes the pile's B-edge quantile, and when a frontier carries more than
+  //    2B edges the threshold drops to its B-edge quantile and a trim launch
+  //    (split = 3) moves the entries at or above it onto the pile. A pile
+  //    entry is live while its bit in fbm is set: a near push of the vertex
+  //    clears it.
   int delta;
   int threshold;
   int prev_threshold;       // threshold before the last rise
-  int split;
+  int split;                // 0 relax, 1 move from the pile, 3 trim the frontier
+  int hshift;               // histogram bin width 2^hshift (budget)
+  int hbase;                // frontier histogram base of the current launch (budget)
+  int pbase;                // pile histogram base (budget)
+  int pad2;
   int pcur;
   unsigned psize[2];
   int pmin[2];              // lower bound of the values on each pile
@@ -187,6 +200,10 @@ struct IterRec {
   long long visited;
   unsigned long long t_ns;
   float feat[kFeatures];
+  int kind;                 // Ctl::split of the launch: 0 relax, 1 move, 3 trim
+  int threshold;            // near/far threshold of the launch (INT_MAX: none)
+  unsigned pile;            // far-pile entries after the launch
+  int pad;
 };
 
 // Everything a relax kernel needs, passed by value.
@@ -199,7 +216,10 @@ struct Ctx {
   int* hwl[3];
   unsigned* htoff[3];
   int* pile[2];             // far piles (SSSP near/far ordering), vertices
+  int* pdeg[2];             // their degrees
+  unsigned pile_cap;        // entries per pile
   unsigned* fbm;            // bit set: vertex is on the current far pile
+  unsigned long long* hist; // 2 x kHistBins edge counts: [0] next frontier, [1] pile
   unsigned* bm[3];
   Ctl* ctl;
   IterRec* recs;

@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kBlock) k_seed(Ctx c) {
 // Per-run parameters, passed by value to k_reset so that queued runs never
 // share a host buffer.
 struct RunParams {
-  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap, delta, hold, stall_ms, then_at, then_variant;
+  int algo, mode, fixed_variant, allowed, src, nsrc, iter_cap, delta, hold, stall_ms, then_at, then_variant, hshift;
   bool operator!=(const RunParams& o) const { return std::memcmp(this, &o, sizeof(RunParams)) != 0; }
 };
 
@@ -137,6 +137,7 @@ __global__ void k_reset(Ctl* ctl, RunParams p) {
   ctl->nsrc = p.nsrc;
   ctl->algo = p.algo;
   ctl->delta = p.delta;
+  ctl->hshift = p.hshift;
   ctl->then_at = p.then_at;
   ctl->then_variant = p.then_variant;
   ctl->hold = p.hold;
@@ -446,6 +447,7 @@ struct i2_graph {
   unsigned* htoff[3] = {nullptr, nullptr, nullptr};
   unsigned* bm[3] = {nullptr, nullptr, nullptr};
   unsigned* fbm = nullptr;  // far-pile bitmap, allocated after bm[2]
+  unsigned long long* hist = nullptr;  // near/far distance histograms, after fbm
   int* pile[2] = {nullptr, nullptr};
   int bm_words = 0;
   bool resident_ok = true;  // cleared if the device refuses the cooperative loop node
@@ -649,6 +651,11 @@ static int finish_setup(i2_graph* g) {
   return compute_stats(g);
 }
 
+// Words of the bitmap block: 4 bitmaps, then (8-byte aligned) the two
+// distance histograms of the budgeted near/far ordering.
+static size_t hist_offset_words(const i2_graph* g) { return (4ull * g->bm_words + 1) & ~1ull; }
+static size_t bm_block_words(const i2_graph* g) { return hist_offset_words(g) + 2ull * 2 * kHistBins; }
+
 static int ensure_workspace(i2_graph* g) {
   if (g->ws_ready) return I2_OK;
   const long long V = g->g.nodes;
@@ -660,10 +667,13 @@ static int ensure_workspace(i2_graph* g) {
     I2_CK(dev_alloc(&g->hwl[k], sizeof(int) * std::max(1, g->gs.nheavy)));
     I2_CK(dev_alloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
   }
+  // one block: the three frontier bitmaps, the far-pile bitmap and the
+  // near/far distance histograms (cleared together before every run)
   unsigned* bm = nullptr;
-  I2_CK(dev_alloc(&bm, sizeof(unsigned) * 4ull * g->bm_words));
+  I2_CK(dev_alloc(&bm, sizeof(unsigned) * bm_block_words(g)));
   for (int k = 0; k < 3; ++k) g->bm[k] = bm + (size_t)k * g->bm_words;
   g->fbm = bm + 3ull * g->bm_words;
+  g->hist = reinterpret_cast<unsigned long long*>(bm + hist_offset_words(g));
   I2_CK(dev_alloc(&g->ctl, sizeof(Ctl)));
   g->rec_cap = (int)std::min<long long>(V + 2, 1 << 16);
   I2_CK(dev_alloc(&g->recs, sizeof(IterRec) * g->rec_cap));
@@ -672,9 +682,13 @@ static int ensure_workspace(i2_graph* g) {
   return I2_OK;
 }
 
+static size_t pile_capacity(const i2_graph* g) { return (size_t)g->g.nodes + 1; }
+
 static int ensure_piles(i2_graph* g) {
   if (g->pile[0]) return I2_OK;
-  for (int k = 0; k < 2; ++k) I2_CK(dev_alloc(&g->pile[k], sizeof(int) * ((size_t)g->g.nodes + 1)));
+  // each pile: nodes + 1 vertices, then their degrees (a full pile sends
+  // vertices to the next frontier instead)
+  for (int k = 0; k < 2; ++k) I2_CK(dev_alloc(&g->pile[k], sizeof(int) * 2 * pile_capacity(g)));
   drop_execs(g);  // graphs bake the context
   return I2_OK;
 }
@@ -744,24 +758,50 @@ static Ctx make_ctx(const i2_graph* g) {
   c.rec_cap = g->rec_cap;
   c.heavy = g->heavy;
   c.bm_words = g->bm_words;
-  c.pile[0] = g->pile[0];
-  c.pile[1] = g->pile[1];
+  c.pile_cap = (unsigned)std::min<size_t>(pile_capacity(g), 0xffffffffu);
+  for (int k = 0; k < 2; ++k) {
+    c.pile[k] = g->pile[k];
+    c.pdeg[k] = g->pile[k] ? g->pile[k] + pile_capacity(g) : nullptr;
+  }
   c.fbm = g->fbm;
+  c.hist = g->hist;
   c.mlp = mlp_device_params();
   c.srcs = nullptr;
   return c;
 }
 
+// Default edge budget of the near/far ordering per SM (I2_SSSP_BUDGET_AUTO):
+// about 7 warp tiles for each resident warp of the edge-balanced kernel.
+// RMAT-22 SSSP (ms, device-timed): plain 2.57; budget 1M 2.95, 2M 2.57,
+// 4M 2.38, 8M 2.60, 16M 2.97 edges.
+constexpr int kBudgetEdgesPerSM = 28672;
+
 // Near/far ordering applies to SSSP with the fixed edge-balanced push only
-// (the style that implements the split launches), and only when the caller
-// asks for it: it relaxes up to 2.2x fewer edges on RMAT graphs, but each
-// split rescans the far pile and every threshold step adds launches, which
-// measured slower than plain frontier-driven relaxation on RMAT, ER and grid
-// graphs of 2^18..2^22 vertices at every step tried.
-static int pick_delta(const i2_graph* g, int algo, int mode, int variant, int requested) {
+// (the style that implements the split launches). Returns the ordering's
+// Ctl::delta: > 0 a fixed threshold step, < 0 minus an edge budget, 0 off.
+// A fixed step relaxes up to 2.2x fewer edges on RMAT graphs, but the step
+// that wins moves with the graph. The edge budget instead keeps each near
+// frontier at about B edges: enough to fill the GPU, few enough that
+// distances settle before their vertices relax.
+static int pick_order(const i2_graph* g, int algo, int mode, int variant, int step, int budget) {
+  if (algo != I2_SSSP || mode != 0 || variant != kVPCta) return 0;
+  if (step > 0) return step;
+  if (budget == I2_SSSP_BUDGET_AUTO) return -std::max(1 << 16, sm_count() * kBudgetEdgesPerSM);
+  if (budget > 0) return -budget;
   (void)g;
-  if (algo != I2_SSSP || mode != 0 || variant != kVPCta || requested <= 0) return 0;
-  return requested;
+  return 0;
+}
+
+// Histogram bin width of the edge budget: the largest power of two not above
+// the smallest weight, the step by which distances grow per hop. (On RMAT-22
+// with weights in [1, 255] most distances from the hub are below 32: the
+// minimum over many paths takes the light edges, so bins sized by the mean
+// weight put the whole budget quantile into the first bin.)
+static int budget_shift(const i2_graph* g) {
+  const int wm = g->gs.wmin > 1 ? g->gs.wmin : 1;
+  int s = 0;
+  while ((2LL << s) <= wm) ++s;  // floor(log2(wmin))
+  return s;
 }
 
 static RunParams make_params(const i2_graph* g, int algo, int mode, int variant, int src, int nsrc, int cap,
@@ -774,6 +814,7 @@ static RunParams make_params(const i2_graph* g, int algo, int mode, int variant,
   p.src = src;
   p.nsrc = nsrc;
   p.delta = delta;
+  p.hshift = budget_shift(g);
   // Test hook: withhold the first barrier release of a resident traversal,
   // so that every block's bounded wait runs out (I2_STALL_MS bounds it).
   const char* hold = std::getenv("I2_TEST_HOLD_BARRIER");
@@ -782,7 +823,7 @@ static RunParams make_params(const i2_graph* g, int algo, int mode, int variant,
   p.stall_ms = stall ? std::max(1, std::atoi(stall)) : 10000;
   // a split launch moves at least one pile entry into a frontier, or learns
   // the pile's exact minimum for the next one
-  p.iter_cap = cap > 0 ? cap : (int)std::min<long long>((long long)g->g.nodes * (delta > 0 ? 3 : 1) + 2, INT_MAX);
+  p.iter_cap = cap > 0 ? cap : (int)std::min<long long>((long long)g->g.nodes * (delta != 0 ? 3 : 1) + 2, INT_MAX);
   return p;
 }
 
@@ -802,7 +843,7 @@ static int add_kernel_node(cudaGraph_t gr, cudaGraphNode_t* node, const cudaGrap
 
 static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, bool resident, const RunParams& rp,
                       ExecEntry** out) {
-  ExecKey key{algo, mode, mode == 0 ? variant : -1, multi ? 1 : 0, rp.delta > 0 ? 1 : 0, resident ? 1 : 0};
+  ExecKey key{algo, mode, mode == 0 ? variant : -1, multi ? 1 : 0, rp.delta != 0 ? 1 : 0, resident ? 1 : 0};
   auto it = g->execs.find(key);
   if (it != g->execs.end()) {
     *out = &it->second;
@@ -823,7 +864,7 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   ms.dst = g->bm[0];
   ms.value = 0;
   ms.elementSize = 4;
-  ms.width = 4ull * g->bm_words;  // frontier and far-pile bitmaps
+  ms.width = bm_block_words(g);  // frontier and far-pile bitmaps, histograms
   ms.height = 1;
   ms.pitch = 0;
   I2_CK(cudaGraphAddMemsetNode(&n_ms, gr, nullptr, 0, &ms));
@@ -856,8 +897,8 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   // branch on the style the previous iteration selected.
   {
     cudaGraphNode_t n;
-    KernelFn fn = resident ? resident_kernel(algo, mode == 0 ? variant : -1, rp.delta > 0)
-                  : mode == 0 ? relax_kernel(algo, variant, rp.delta > 0)
+    KernelFn fn = resident ? resident_kernel(algo, mode == 0 ? variant : -1, rp.delta != 0)
+                  : mode == 0 ? relax_kernel(algo, variant, rp.delta != 0)
                               : dispatch_kernel(algo);
     st = add_kernel_node(body, &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
     if (st) return st;
@@ -898,7 +939,7 @@ static int launch_exec(i2_graph* g, ExecEntry* e, const RunParams& rp, cudaStrea
 
 // Reset the bitmaps and the control block on the stream (host-driven paths).
 static int prepare_run(i2_graph* g, cudaStream_t s, const RunParams& rp) {
-  I2_CK(cudaMemsetAsync(g->bm[0], 0, sizeof(unsigned) * 4ull * g->bm_words, s));
+  I2_CK(cudaMemsetAsync(g->bm[0], 0, sizeof(unsigned) * bm_block_words(g), s));
   k_reset<<<1, 32, 0, s>>>(g->ctl, rp);
   I2_CK(cudaGetLastError());
   return I2_OK;
@@ -921,7 +962,7 @@ static int run_host_loop(i2_graph* g, cudaStream_t s, int algo, bool multi, doub
     // the last launch's decision: another frontier, a near/far split, the
     // compress launch of union-find, or the end (including the iteration cap)
     if (!h->go || (h->status & kStatusIterCap)) break;
-    KernelFn fn = relax_kernel(algo, h->variant, h->delta > 0);
+    KernelFn fn = relax_kernel(algo, h->variant, h->delta != 0);
     I2_CK(cudaEventRecord(g->ev2, s));
     fn<<<grid_for(fn, g->blocks_per_sm), kBlock, 0, s>>>(c);
     I2_CK(cudaGetLastError());
@@ -983,6 +1024,7 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     o.variant = kVPWarp;
     o.then_at = 0;
     o.sssp_delta = 0;
+    o.sssp_budget = 0;
   }
   int mode = 0, variant = o.variant;
   if (variant == I2_AUTO_HEURISTIC) mode = 1;
@@ -1019,8 +1061,8 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
     }
     I2_CK(cudaMemcpyAsync(g->srcs, srcs_host, sizeof(int) * nsrc, cudaMemcpyHostToDevice, s));
   }
-  const int delta = pick_delta(g, algo, mode, variant, o.sssp_delta);
-  if (delta > 0) {
+  const int delta = pick_order(g, algo, mode, variant, o.sssp_delta, o.sssp_budget);
+  if (delta != 0) {
     st = ensure_piles(g);
     if (st) return st;
   }

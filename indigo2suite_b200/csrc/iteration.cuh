@@ -98,12 +98,102 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
   }
 }
 
+// Edge budget of the SSSP near/far ordering (whole block; kBlock bins): the
+// first bin at which each histogram's running edge count reaches the budget
+// (kHistBins if it never does): [0] the next frontier's, [1] the pile's. The
+// next frontier's histogram is then cleared for the next launch's pushes.
+static_assert(kHistBins == kBlock, "one histogram bin per thread");
+static __device__ void budget_quantiles(const Ctx& c, int* q) {
+  __shared__ unsigned long long part[kBlock / kWarp];
+  __shared__ int sq[2];
+  const unsigned long long B = (unsigned long long)(-(long long)c.ctl->delta);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int which = 0; which < 2; ++which) {
+    unsigned long long* h = c.hist + which * kHistBins;
+    const unsigned long long x = *(volatile unsigned long long*)&h[threadIdx.x];
+    unsigned long long incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) part[wid] = incl;
+    if (threadIdx.x == 0) sq[which] = kHistBins;
+    __syncthreads();
+    for (int w = 0; w < wid; ++w) incl += part[w];
+    if (incl >= B && incl - x < B) sq[which] = threadIdx.x;
+    __syncthreads();
+  }
+  q[0] = sq[0];
+  q[1] = sq[1];
+  c.hist[threadIdx.x] = 0ull;
+}
+
+// Thread 0 of the last block, edge budget: the next launch of the ordering.
+// `q` are the histogram quantiles, `n`/`e` the next frontier's entries and
+// edges. Returns whether another launch follows; *clear_pile is set when the
+// pile histogram must be cleared (a move rebuilds it from the entries it keeps).
+static __device__ int budget_next(const Ctx& c, const int* q, long long n, unsigned e, int nxt, int* clear_pile) {
+  Ctl* ctl = c.ctl;
+  const long long B = -(long long)ctl->delta;
+  const int shift = ctl->hshift;
+  const int was = ctl->split;
+  const int p = ctl->pcur;
+  int cond = n > 0;
+  *clear_pile = 0;
+  if (was == 1) {  // the move emptied pile p onto the other one
+    ctl->psize[p] = 0;
+    ctl->pmin[p] = kInf;
+    ctl->pcur = 1 - p;
+  }
+  ctl->split = 0;
+  const int np = ctl->pcur;
+  // move next when the frontier is empty, or so small that its last
+  // iterations would cost more launches than edges (it is carried along)
+  if (*(volatile unsigned*)&ctl->psize[np] > 0 && (n == 0 || (was == 0 && (long long)e * 16 < B))) {
+    // at the budget's quantile of the pile (and above the pile's lower bound,
+    // so that a live entry moves, or the move learns the bound)
+    const int pm = *(volatile int*)&ctl->pmin[np];
+    long long T = q[1] < kHistBins ? (long long)ctl->pbase + ((long long)(q[1] + 1) << shift) : (long long)kInf;
+    if (pm != kInf) T = max(T, (long long)pm + 1);
+    T = min(T, (long long)kInf);
+    ctl->prev_threshold = ctl->threshold;
+    ctl->threshold = (int)T;
+    int lo = pm != kInf ? pm : ctl->pbase;  // the smallest value the move can carry
+    if (n > 0) lo = min(lo, *(volatile int*)&ctl->slot[nxt].mindist);
+    ctl->hbase = lo;
+    ctl->pbase = (int)T;                       // kept values are at or above T
+    ctl->split = 1;
+    *clear_pile = 1;
+    return 1;
+  }
+  if (n > 0 && was != 3 && (long long)e > 2 * B && q[0] < kHistBins) {
+    const long long T = (long long)ctl->hbase + ((long long)(q[0] + 1) << shift);
+    if (T < (long long)ctl->threshold) {  // trim the next frontier to about B edges
+      ctl->threshold = (int)T;
+      ctl->split = 3;
+    }
+  }
+  ctl->hbase = *(volatile int*)&ctl->slot[nxt].mindist;
+  return cond;
+}
+
 // Last block of a relax launch: record the launch, advance the iteration and
 // decide whether the loop continues.
 static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, int old) {
-  __shared__ int s_cond, s_force;
+  __shared__ int s_cond, s_force, s_clear;
+  __shared__ int s_q[2];
   Ctl* ctl = c.ctl;
   if (ctl->variant == kUnionFind && ctl->uf_phase == 0) uf_sample_giant(c);  // whole block
+  if (threadIdx.x == 0) s_clear = 0;
+  if (ctl->delta < 0) {
+    int q[2];
+    budget_quantiles(c, q);
+    if (threadIdx.x == 0) {
+      s_q[0] = q[0];
+      s_q[1] = q[1];
+    }
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     const unsigned long long t1 = globaltimer();
     const unsigned long long dt = t1 - ctl->tstart;
@@ -121,6 +211,9 @@ static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, i
       r.visited = *(volatile long long*)&ctl->visited;
       r.t_ns = dt;
       for (int k = 0; k < kFeatures; ++k) r.feat[k] = ctl->feat[k];
+      r.kind = ctl->split;
+      r.threshold = ctl->threshold;
+      r.pile = ctl->delta != 0 ? *(volatile unsigned*)&ctl->psize[ctl->split == 1 ? 1 - ctl->pcur : ctl->pcur] : 0u;
     }
     Slot& so = ctl->slot[old];
     so.packed = 0;
@@ -135,7 +228,9 @@ static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, i
     volatile Slot* sn = &ctl->slot[nxt];
     const long long n = slot_size(sn->packed);
     int cond = n > 0;
-    if (ctl->delta > 0) {
+    if (ctl->delta < 0) {
+      cond = budget_next(c, s_q, n, slot_edges(sn->packed), nxt, &s_clear);
+    } else if (ctl->delta > 0) {
       if (ctl->split) {  // this launch emptied pile pcur onto the other one
         const int p = ctl->pcur;
         ctl->psize[p] = 0;
@@ -171,6 +266,7 @@ static __device__ void finish_iteration(const Ctx& c, int i, int cur, int nxt, i
     s_force = force;
   }
   __syncthreads();
+  if (s_clear) c.hist[kHistBins + threadIdx.x] = 0ull;  // read above; the move rebuilds it
   select_next(c, i + 1, nxt, s_cond != 0, s_force);
 }
 

@@ -28,6 +28,7 @@
 #include <cooperative_groups/reduce.h>
 #include <cooperative_groups/scan.h>
 #include <cub/block/block_scan.cuh>
+#include <type_traits>
 #include "common.cuh"
 
 namespace i2 {
@@ -171,31 +172,91 @@ __device__ __forceinline__ void direct_append(unsigned long long* packed, int* l
   off[pos] = (unsigned)(base & 0xffffffffu) + (unsigned)pre;
 }
 
-// Append v to a far pile; the threads that append together share one atomic.
-__device__ __forceinline__ void pile_append(int* pile, unsigned* size, int v) {
+// Append v (degree deg) to far pile p; the threads that append together share
+// one atomic. False when the pile is full (the size counter may then pass the
+// capacity: readers clamp it).
+__device__ __forceinline__ bool pile_append(const Ctx& c, int p, int v, int deg) {
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(size, (unsigned)g.size());
+  if (g.thread_rank() == 0) base = atomicAdd(&c.ctl->psize[p], (unsigned)g.size());
   base = g.shfl(base, 0);
-  pile[base + g.thread_rank()] = v;
+  const unsigned pos = base + g.thread_rank();
+  if (pos >= c.pile_cap || pos < base) return false;
+  c.pile[p][pos] = v;
+  c.pdeg[p][pos] = deg;
+  return true;
+}
+
+// Per-block distance histograms of the budgeted near/far ordering (shared
+// memory; h null when off): h[0..kHistBins) for the next frontier (every near
+// push adds the vertex's degree to the bin of its value, (val - fbase) >> shift
+// clamped to the bins), h[kHistBins..) for the far pile (every new pile entry,
+// relative to pbase). The block adds its bins to the device histograms once
+// per launch.
+struct Hists {
+  unsigned* h;
+  int fbase;
+  int pbase;
+  int shift;
+};
+
+__device__ __forceinline__ int hist_bin(int val, int base, int shift) {
+  const long long off = ((long long)val - (long long)base) >> shift;
+  return (int)(off < 0 ? 0 : (off >= kHistBins ? kHistBins - 1 : off));
+}
+
+__device__ __forceinline__ void hist_near(const Hists& hs, int val, int deg) {
+  atomicAdd(&hs.h[hist_bin(val, hs.fbase, hs.shift)], (unsigned)deg);
+}
+
+__device__ __forceinline__ void hist_far(const Hists& hs, int val, int deg) {
+  atomicAdd(&hs.h[kHistBins + hist_bin(val, hs.pbase, hs.shift)], (unsigned)deg);
 }
 
 // Defer v (new value val, at or above the threshold) to the current far pile.
-// The pile's bitmap keeps one entry per vertex: a vertex already on the pile
-// only lowers the pile's minimum. Vertices without edges are never deferred.
-__device__ __forceinline__ void defer_vertex(const Ctx& c, Acc& a, int v, int val, int old) {
-  if (old == kInf) a.visited++;
-  a.fmin = min(a.fmin, val);
+// The pile's bitmap keeps one live entry per vertex: a vertex already on the
+// pile only lowers the pile's minimum. Vertices without edges are never
+// deferred. With a warp stage the entry is staged (published by warp_flush
+// with one atomic per flush); without one it is appended at once. False when
+// the pile is full: the caller then pushes v into the next frontier, which is
+// always valid. With the edge budget (hs) new entries are histogrammed.
+struct WarpStage;
+__device__ __forceinline__ bool stage_far(const Ctx& c, WarpStage* ws, int v, int deg);
+
+__device__ __forceinline__ bool defer_vertex(const Ctx& c, Acc& a, int v, int val, WarpStage* ws = nullptr,
+                                             const Hists* hs = nullptr) {
   const unsigned bit = 1u << (v & 31);
   unsigned* w = &c.fbm[v >> 5];
-  if (*(volatile unsigned*)w & bit) return;
-  if (atomicOr(w, bit) & bit) return;
-  if (c.g.nindex[v + 1] == c.g.nindex[v]) {
-    atomicAnd(w, ~bit);
-    return;
+  if (*(volatile unsigned*)w & bit) {
+    a.fmin = min(a.fmin, val);
+    return true;
   }
-  const int p = c.ctl->pcur;
-  pile_append(c.pile[p], &c.ctl->psize[p], v);
+  if (atomicOr(w, bit) & bit) {
+    a.fmin = min(a.fmin, val);
+    return true;
+  }
+  const int deg = c.g.nindex[v + 1] - c.g.nindex[v];
+  if (deg == 0) {
+    atomicAnd(w, ~bit);
+    return true;
+  }
+  if (ws ? !stage_far(c, ws, v, deg) : !pile_append(c, c.ctl->pcur, v, deg)) {
+    atomicAnd(w, ~bit);
+    return false;
+  }
+  a.fmin = min(a.fmin, val);
+  if (hs) hist_far(*hs, val, deg);
+  return true;
+}
+
+// A near push of v supersedes v's pile entry, if any (its bit is cleared, so
+// the entry is dropped when the pile is next read). Needed where the
+// threshold may fall (the edge budget): there a pile entry cannot be told
+// stale from its value alone.
+__device__ __forceinline__ void unpile(const Ctx& c, int v) {
+  const unsigned bit = 1u << (v & 31);
+  unsigned* w = &c.fbm[v >> 5];
+  if (*(volatile unsigned*)w & bit) atomicAnd(w, ~bit);
 }
 
 // Record vertex v (degree deg >= 1) in the next frontier. The bitmap bit is
@@ -515,8 +576,8 @@ __device__ __forceinline__ bool block_epilogue(const Ctx& c, S& s, const Acc& a,
     if (r.maxdeg) atomicMax(&sl.maxdeg, r.maxdeg);
     if (r.mindist != kInf) atomicMin(&sl.mindist, r.mindist);
     if (r.visited) atomicAdd((unsigned long long*)&c.ctl->visited, (unsigned long long)r.visited);
-    // far pushes of a relax launch go onto pile pcur, a split's onto the other
-    if (r.fmin != kInf) atomicMin(&c.ctl->pmin[c.ctl->split ? 1 - c.ctl->pcur : c.ctl->pcur], r.fmin);
+    // far pushes of a relax or trim launch go onto pile pcur, a move's onto the other
+    if (r.fmin != kInf) atomicMin(&c.ctl->pmin[c.ctl->split == 1 ? 1 - c.ctl->pcur : c.ctl->pcur], r.fmin);
     __threadfence();
     const unsigned t = atomicAdd(&c.ctl->done, 1u);
     s.last = (t == gridDim.x - 1);
@@ -656,14 +717,25 @@ __device__ __forceinline__ void warp_stage_entry(const Ctx& c, WarpStage& ws, Ac
   if (deg >= c.heavy) direct_append(&c.ctl->slot[nxt].hpacked, c.hwl[nxt], c.htoff[nxt], v, heavy_tiles(deg));
 }
 
+// Stage a far-pile entry of the near/far ordering: kept in the warp's queue
+// as ~v (negative) beside its degree, and published by warp_flush<true>.
+// Without room in the queue it is appended at once.
+__device__ __forceinline__ bool stage_far(const Ctx& c, WarpStage* ws, int v, int deg) {
+  const int p = atomicAdd(&ws->n, 1);
+  if (p < kWarpQueue) {
+    ws->q[p] = ~v;
+    ws->qd[p] = deg;
+    return true;
+  }
+  return pile_append(c, c.ctl->pcur, v, deg);
+}
+
 template <bool DEFER>
 __device__ __forceinline__ void warp_push_vertex(const Ctx& c, WarpStage& ws, Acc& a, int nxt, int v, int val,
-                                                 int old, int thr) {
-  if (DEFER && val >= thr) {
-    defer_vertex(c, a, v, val, old);
-    return;
-  }
+                                                 int old, int thr, const Hists& hs) {
   if (old == kInf) a.visited++;
+  if (DEFER && val >= thr && defer_vertex(c, a, v, val, &ws, hs.h ? &hs : nullptr)) return;
+  if (DEFER && hs.h) unpile(c, v);
   a.mindist = min(a.mindist, val);
   const unsigned bit = 1u << (v & 31);
   unsigned* w = &c.bm[nxt][v >> 5];
@@ -674,10 +746,16 @@ __device__ __forceinline__ void warp_push_vertex(const Ctx& c, WarpStage& ws, Ac
     atomicAnd(w, ~bit);
     return;
   }
+  if (DEFER && hs.h) hist_near(hs, val, deg);
   warp_stage_entry(c, ws, a, nxt, v, deg);
 }
 
-// Publish the warp's staged entries (warp-uniform call).
+// Publish the warp's staged entries (warp-uniform call): one packed atomic
+// reserves positions and edge offsets in the next frontier for all of them.
+// DEFER: the queue also holds far-pile entries (negative, ~v); they go onto
+// the current pile with one more atomic, and the frontier entries are
+// compacted. Far entries that find the pile full join the next frontier.
+template <bool DEFER = false>
 __device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt) {
   constexpr int kPer = kWarpQueue / kWarp;
   __syncwarp();
@@ -685,24 +763,101 @@ __device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt)
   __syncwarp();
   if (n == 0) return;
   const int lane = threadIdx.x & 31;
-  int d[kPer];
-  int sum = 0;
+  if constexpr (DEFER) {
+    int nf = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int j = lane * kPer + i;
+      nf += (j < n && ws.q[j] < 0) ? 1 : 0;
+    }
+    int fincl = nf;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, fincl, o);
+      if (lane >= o) fincl += y;
+    }
+    const int ftot = __shfl_sync(0xffffffffu, fincl, 31);
+    if (ftot) {
+      const int p = c.ctl->pcur;
+      unsigned pb = 0;
+      if (lane == 0) pb = atomicAdd(&c.ctl->psize[p], (unsigned)ftot);
+      pb = __shfl_sync(0xffffffffu, pb, 0);
+      unsigned k = pb + (unsigned)(fincl - nf);
+      for (int i = 0; i < kPer; ++i) {
+        const int j = lane * kPer + i;
+        if (j < n && ws.q[j] < 0) {
+          const int v = ~ws.q[j];
+          if (k < c.pile_cap && k >= pb) {
+            c.pile[p][k] = v;
+            c.pdeg[p][k] = ws.qd[j];
+          } else {  // pile full: the vertex joins the next frontier instead
+            const unsigned bit = 1u << (v & 31);
+            atomicAnd(&c.fbm[v >> 5], ~bit);
+            if (!(atomicOr(&c.bm[nxt][v >> 5], bit) & bit)) {
+              ws.q[j] = v;
+              if (ws.qd[j] >= c.heavy)
+                direct_append(&c.ctl->slot[nxt].hpacked, c.hwl[nxt], c.htoff[nxt], v, heavy_tiles(ws.qd[j]));
+            }
+          }
+          ++k;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if constexpr (!DEFER) {
+    int d[kPer];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int j = lane * kPer + i;
+      d[i] = sum;
+      sum += j < n ? ws.qd[j] : 0;
+    }
+    int incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - sum;
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long base = 0;
+    if (lane == 0) {
+      base = atomicAdd(&c.ctl->slot[nxt].packed, ((unsigned long long)n << 32) | (unsigned)tot);
+      ws.n = 0;
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const int b = (int)(base >> 32);
+    const unsigned eb = (unsigned)(base & 0xffffffffu);
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int j = lane * kPer + i;
+      if (j < n) {
+        c.wl[nxt][b + j] = ws.q[j];
+        c.woff[nxt][b + j] = eb + (unsigned)(excl + d[i]);
+      }
+    }
+    __syncwarp();
+    return;
+  }
+  // frontier entries: count and degree prefix in one 64-bit scan
+  unsigned long long d[kPer];
+  unsigned long long sum = 0;
 #pragma unroll
   for (int i = 0; i < kPer; ++i) {
     const int j = lane * kPer + i;
     d[i] = sum;
-    sum += j < n ? ws.qd[j] : 0;
+    if (j < n && ws.q[j] >= 0) sum += (1ull << 32) | (unsigned)ws.qd[j];
   }
-  int incl = sum;
+  unsigned long long incl = sum;
   for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
   }
-  const int excl = incl - sum;
-  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+  const unsigned long long excl = incl - sum;
+  const unsigned long long tot = __shfl_sync(0xffffffffu, incl, 31);
   unsigned long long base = 0;
   if (lane == 0) {
-    base = atomicAdd(&c.ctl->slot[nxt].packed, ((unsigned long long)n << 32) | (unsigned)tot);
+    if (tot) base = atomicAdd(&c.ctl->slot[nxt].packed, tot);
     ws.n = 0;
   }
   base = __shfl_sync(0xffffffffu, base, 0);
@@ -711,9 +866,10 @@ __device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt)
 #pragma unroll
   for (int i = 0; i < kPer; ++i) {
     const int j = lane * kPer + i;
-    if (j < n) {
-      c.wl[nxt][b + j] = ws.q[j];
-      c.woff[nxt][b + j] = eb + (unsigned)(excl + d[i]);
+    if (j < n && ws.q[j] >= 0) {
+      const unsigned long long x = excl + d[i];
+      c.wl[nxt][b + (int)(x >> 32)] = ws.q[j];
+      c.woff[nxt][b + (int)(x >> 32)] = eb + (unsigned)(x & 0xffffffffu);
     }
   }
   __syncwarp();
@@ -721,7 +877,8 @@ __device__ __forceinline__ void warp_flush(const Ctx& c, WarpStage& ws, int nxt)
 
 template <int ALG, bool DEFER>
 __device__ __forceinline__ void warp_relax_batch(const Ctx& c, WarpStage& ws, Acc& a, int nxt, const int* du,
-                                                 const int* nv, const int* wv, const bool* ok, int thr) {
+                                                 const int* nv, const int* wv, const bool* ok, int thr,
+                                                 const Hists& hs) {
   int cand[kEdgesPerThread], cur[kEdgesPerThread];
 #pragma unroll
   for (int r = 0; r < kEdgesPerThread; ++r) {
@@ -732,7 +889,7 @@ __device__ __forceinline__ void warp_relax_batch(const Ctx& c, WarpStage& ws, Ac
   for (int r = 0; r < kEdgesPerThread; ++r) {
     if (cand[r] < cur[r]) {
       const int old = atomicMin(&c.dist[nv[r]], cand[r]);
-      if (cand[r] < old) warp_push_vertex<DEFER>(c, ws, a, nxt, nv[r], cand[r], old, thr);
+      if (cand[r] < old) warp_push_vertex<DEFER>(c, ws, a, nxt, nv[r], cand[r], old, thr, hs);
     }
   }
 }
@@ -751,18 +908,61 @@ struct EBShared {
   WarpStage wss[kWarpsPerBlock];
 };
 
-// Split launch of the SSSP near/far ordering (F_i is empty, the far pile is
-// not, the threshold has just risen from T0 to T). Each pile entry with a
-// distance below T moves into F_{i+1}; one at or above T moves onto the other
-// pile. An entry whose distance is below T0 was lowered after it was deferred
-// by a push that put it into a frontier (values only fall and the threshold
-// only rises), so it has been relaxed with that distance and is dropped.
-__device__ __forceinline__ bool body_split(const Ctx& c, EBShared& sh, int i, int cur, int nxt, int old) {
+// Near/far ordering: the per-block distance histogram of the edge budget.
+static_assert(kHistBins == kBlock, "one histogram bin per thread");
+struct EBSharedFar : EBShared {
+  unsigned hist[2 * kHistBins];  // next frontier, far pile
+};
+
+template <bool DEFER>
+using EBSharedT = typename std::conditional<DEFER, EBSharedFar, EBShared>::type;
+
+// Budgeted near/far ordering, start of a launch (block-uniform): clear the
+// block's histograms. End of a launch: add them to the device histograms.
+__device__ __forceinline__ void block_hist_begin(unsigned* h) {
+  h[threadIdx.x] = 0u;
+  h[kHistBins + threadIdx.x] = 0u;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void block_hist_end(const unsigned* h, unsigned long long* dst) {
+  __syncthreads();
+  const unsigned x = h[threadIdx.x], y = h[kHistBins + threadIdx.x];
+  if (x) atomicAdd(&dst[threadIdx.x], (unsigned long long)x);
+  if (y) atomicAdd(&dst[kHistBins + threadIdx.x], (unsigned long long)y);
+}
+
+// Launches of the SSSP near/far ordering other than relaxations (Ctl::split):
+//  1 move: F_i is empty, the pile is not, and the threshold has just risen
+//    from T0 to T. Each live pile entry with a distance below T moves into
+//    F_{i+1}; one at or above T moves onto the other pile. Fixed step: an entry
+//    whose distance is below T0 was lowered after it was deferred by a push
+//    that put it into a frontier (values only fall and the threshold only
+//    rises), so it has been relaxed with that distance and is dropped. Edge
+//    budget: an entry is live while its fbm bit is set (a near push clears it)
+//    and dead entries are dropped; the first copy of a vertex that moves clears
+//    the bit, so it moves once; the kept entries are histogrammed anew (base T)
+//    for the next move.
+//  3 trim (edge budget): F_i carries more than twice the budget and the
+//    threshold has just fallen to T; entries below T move into F_{i+1}, the
+//    others onto the pile (nothing is relaxed).
+// The loop is block-uniform: a block appends the entries it keeps with one
+// atomic per pass (a single pile counter takes every block's appends).
+__device__ __forceinline__ bool body_split(const Ctx& c, EBSharedFar& sh, int i, int cur, int nxt, int old) {
+  __shared__ int s_keep[kWarpsPerBlock];
+  __shared__ unsigned s_kbase;
   EpiStage& s = sh.s;
   Ctl* ctl = c.ctl;
+  const int mode = ctl->split;
+  const bool budget = ctl->delta < 0;
   const int p = ctl->pcur;
-  const unsigned n = ctl->psize[p];
+  const unsigned long long P = ctl->slot[cur].packed;
+  // F_i's entries first (a trim's input, or what an early move carries), then
+  // the pile's (a move)
+  const unsigned nf = (unsigned)slot_size(P);
+  const unsigned n = nf + (mode == 1 ? min(ctl->psize[p], c.pile_cap) : 0u);
   const int T = ctl->threshold, T0 = ctl->prev_threshold;
+  const Hists hs = budget ? Hists{sh.hist, ctl->hbase, ctl->pbase, ctl->hshift} : Hists{};
   const int active = active_blocks(c, old, ((long long)n + kBlock - 1) / kBlock);
   if (blockIdx.x >= active) {
     return idle_epilogue(c, s, i, cur, nxt, old);
@@ -770,37 +970,122 @@ __device__ __forceinline__ bool body_split(const Ctx& c, EBShared& sh, int i, in
   if (threadIdx.x == 0) s.last = 0;
   Acc a;
   acc_init(a);
+  if (budget) block_hist_begin(sh.hist);
   clear_old(c, old, active);
-  const int lane = threadIdx.x & 31;
-  WarpStage& ws = sh.wss[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  WarpStage& ws = sh.wss[wid];
   if (lane == 0) ws.n = 0;
   __syncwarp();
-  const int* from = c.pile[p];
-  int* to = c.pile[1 - p];
-  const unsigned stride = (unsigned)active * kBlock;
-  // warp-uniform loop: every lane takes part in the flushes
-  for (unsigned base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += stride) {
-    const unsigned j = base + lane;
-    if (j < n) {
-      const int v = from[j];
-      const unsigned bit = 1u << (v & 31);
-      const int d = c.dist[v];
-      if (d < T) {
-        atomicAnd(&c.fbm[v >> 5], ~bit);
-        if (d >= T0) {
-          atomicOr(&c.bm[nxt][v >> 5], bit);
-          a.mindist = min(a.mindist, d);
-          warp_stage_entry(c, ws, a, nxt, v, c.g.nindex[v + 1] - c.g.nindex[v]);
+  const int* pv = c.pile[p];
+  const int* pd = c.pdeg[p];
+  // kR entries per thread and pass (L2-coherent loads: other blocks wrote
+  // these arrays in earlier iterations). kR = 4 measured no faster on RMAT-22
+  // moves and slower on trims (fewer blocks share a small frontier).
+  constexpr int kR = 1;
+  const unsigned stride = (unsigned)active * kBlock * kR;
+  for (unsigned base = blockIdx.x * kBlock * kR; base < n; base += stride) {
+    int v[kR], d[kR], deg[kR];
+    unsigned fw[kR];
+    bool in[kR], front[kR];
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const unsigned j = base + (unsigned)r * kBlock + threadIdx.x;
+      in[r] = j < n;
+      front[r] = j < nf;
+      v[r] = in[r] ? (front[r] ? __ldcg(&c.wl[cur][j]) : __ldcg(&pv[j - nf])) : 0;
+      deg[r] = 0;
+      if (in[r]) {
+        if (front[r]) {
+          const unsigned w1 = j + 1 < nf ? __ldcg(&c.woff[cur][j + 1]) : slot_edges(P);
+          deg[r] = (int)(w1 - __ldcg(&c.woff[cur][j]));
+        } else {
+          deg[r] = __ldcg(&pd[j - nf]);
         }
-      } else {
-        a.fmin = min(a.fmin, d);
-        pile_append(to, &ctl->psize[1 - p], v);
       }
     }
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      fw[r] = in[r] && !front[r] ? __ldcg(&c.fbm[v[r] >> 5]) : 0u;
+      d[r] = in[r] ? __ldcg(&c.dist[v[r]]) : 0;
+    }
+    bool keep[kR];
+    int nkeep = 0;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      keep[r] = false;
+      if (!in[r]) continue;
+      const unsigned bit = 1u << (v[r] & 31);
+      if (front[r]) {  // a frontier entry: below T it stays near, else it goes onto the pile
+        if (d[r] >= T && defer_vertex(c, a, v[r], d[r], &ws, budget ? &hs : nullptr)) {
+          // on the pile
+        } else if (!(atomicOr(&c.bm[nxt][v[r] >> 5], bit) & bit)) {
+          a.mindist = min(a.mindist, d[r]);
+          if (budget) hist_near(hs, d[r], deg[r]);
+          warp_stage_entry(c, ws, a, nxt, v[r], deg[r]);
+        }
+      } else if (budget) {  // a pile entry (move), live while its fbm bit is set
+        if (fw[r] & bit) {
+          if (d[r] < T) {
+            if ((atomicAnd(&c.fbm[v[r] >> 5], ~bit) & bit) && !(atomicOr(&c.bm[nxt][v[r] >> 5], bit) & bit)) {
+              a.mindist = min(a.mindist, d[r]);
+              hist_near(hs, d[r], deg[r]);
+              warp_stage_entry(c, ws, a, nxt, v[r], deg[r]);
+            }
+          } else {
+            keep[r] = true;
+            a.fmin = min(a.fmin, d[r]);
+            hist_far(hs, d[r], deg[r]);
+          }
+        }
+      } else if (d[r] < T) {  // fixed step
+        atomicAnd(&c.fbm[v[r] >> 5], ~bit);
+        if (d[r] >= T0) {
+          atomicOr(&c.bm[nxt][v[r] >> 5], bit);
+          a.mindist = min(a.mindist, d[r]);
+          warp_stage_entry(c, ws, a, nxt, v[r], deg[r]);
+        }
+      } else {
+        keep[r] = true;
+        a.fmin = min(a.fmin, d[r]);
+      }
+      nkeep += keep[r] ? 1 : 0;
+    }
+    if (mode == 1) {  // kept entries onto the other pile: one atomic per block pass
+      int incl = nkeep;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) s_keep[wid] = incl;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kWarpsPerBlock; ++w) {
+          const int x = s_keep[w];
+          s_keep[w] = t;
+          t += x;
+        }
+        s_kbase = t ? atomicAdd(&ctl->psize[1 - p], (unsigned)t) : 0u;
+      }
+      __syncthreads();
+      unsigned pos = s_kbase + (unsigned)s_keep[wid] + (unsigned)(incl - nkeep);
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        if (keep[r]) {
+          if (pos < c.pile_cap) {  // kept entries <= pile entries <= capacity
+            c.pile[1 - p][pos] = v[r];
+            c.pdeg[1 - p][pos] = deg[r];
+          }
+          ++pos;
+        }
+      }
+      __syncthreads();  // s_keep and s_kbase are rewritten by the next pass
+    }
     __syncwarp();
-    if (ws.n >= kWarpQueue - kWarp) warp_flush(c, ws, nxt);
+    if (ws.n >= kWarpQueue - kR * kWarp) warp_flush<true>(c, ws, nxt);
   }
-  warp_flush(c, ws, nxt);
+  warp_flush<true>(c, ws, nxt);
+  if (budget) block_hist_end(sh.hist, c.hist);
   __syncthreads();
   return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
@@ -808,16 +1093,20 @@ __device__ __forceinline__ bool body_split(const Ctx& c, EBShared& sh, int i, in
 // DEFER: SSSP near/far ordering (pushes at or above the threshold go onto the
 // far pile, and split launches refill the frontier from it).
 template <int ALG, bool DEFER = false>
-__device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBShared& sh) {
+__device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBSharedT<DEFER>& sh) {
   static_assert(!DEFER || ALG == kSSSP, "near/far ordering is for SSSP");
   EpiStage& s = sh.s;
   block_prologue(c);
   const int i = c.ctl->iter;
   const int cur = i % 3, nxt = (i + 1) % 3, old = (i + 2) % 3;
-  if (DEFER && c.ctl->split) {
-    return body_split(c, sh, i, cur, nxt, old);
+  if constexpr (DEFER) {
+    if (c.ctl->split) return body_split(c, sh, i, cur, nxt, old);
   }
   const int thr = DEFER ? c.ctl->threshold : kInf;
+  Hists hs{};
+  if constexpr (DEFER) {
+    if (c.ctl->delta < 0) hs = Hists{sh.hist, c.ctl->hbase, c.ctl->pbase, c.ctl->hshift};
+  }
   const unsigned long long P = c.ctl->slot[cur].packed;
   const int n = slot_size(P);
   const unsigned total = slot_edges(P);
@@ -829,6 +1118,7 @@ __device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBShared& sh) {
   if (threadIdx.x == 0) s.last = 0;
   Acc a;
   acc_init(a);
+  if (DEFER && hs.h) block_hist_begin(hs.h);
   clear_old(c, old, active);
   const int lane = threadIdx.x & 31;
   WarpStage& ws = sh.wss[threadIdx.x >> 5];
@@ -890,14 +1180,15 @@ __device__ __forceinline__ bool body_edge_balanced(const Ctx& c, EBShared& sh) {
           ok[r] = Op<ALG>::valid(du[r]);
         }
       }
-      warp_relax_batch<ALG, DEFER>(c, ws, a, nxt, du, nv, wv, ok, thr);
+      warp_relax_batch<ALG, DEFER>(c, ws, a, nxt, du, nv, wv, ok, thr, hs);
       // the next tile starts at e1: its first entry is the last one with offset <= e1
       j += (ws.off[m] == e1) ? m : m - 1;
       __syncwarp();
-      if (ws.n >= kWarpQueue / 2) warp_flush(c, ws, nxt);
+      if (ws.n >= kWarpQueue / 2) warp_flush<DEFER>(c, ws, nxt);
     }
   }
-  warp_flush(c, ws, nxt);
+  warp_flush<DEFER>(c, ws, nxt);
+  if (DEFER && hs.h) block_hist_end(hs.h, c.hist);
   __syncthreads();
   return block_epilogue(c, s, a, i, cur, nxt, old, active);
 }
@@ -1311,9 +1602,9 @@ static __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_mis(Ctx
   body_mis(c, sh);
 }
 
-// Edge-balanced SSSP push with near/far ordering (Ctl::delta > 0).
+// Edge-balanced SSSP push with near/far ordering (Ctl::delta != 0).
 static __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_near_far(Ctx c) {
-  __shared__ EBShared sh;
+  __shared__ EBSharedFar sh;
   body_edge_balanced<kSSSP, true>(c, sh);
 }
 
@@ -1341,9 +1632,10 @@ __global__ void __launch_bounds__(kBlock) relax_pull(Ctx c) {
   body_pull<ALG, FRONTIER>(c, s);
 }
 
+template <bool DEFER = false>
 union AnyShared {
   Stage st;
-  EBShared eb;
+  EBSharedT<DEFER> eb;
 };
 
 // ---------------------------------------------------------------------------
@@ -1376,7 +1668,7 @@ __device__ __forceinline__ void grid_wait(Ctl* ctl, unsigned gen) {
 }
 
 template <int ALG, int VAR, bool DEFER>
-__device__ __forceinline__ bool run_body(const Ctx& c, AnyShared& sh) {
+__device__ __forceinline__ bool run_body(const Ctx& c, AnyShared<DEFER>& sh) {
   if constexpr (ALG == kMIS) {
     return body_mis(c, sh.eb);  // one style
   } else {
@@ -1401,7 +1693,7 @@ __device__ __forceinline__ bool run_body(const Ctx& c, AnyShared& sh) {
 // iteration by the previous one (heuristic or learned selector).
 template <int ALG, int VAR, bool DEFER = false>
 __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_resident(Ctx c) {
-  __shared__ AnyShared sh;
+  __shared__ AnyShared<DEFER> sh;
   __shared__ int s_go;
   Ctl* ctl = c.ctl;
   if (threadIdx.x == 0) s_go = !(*(volatile int*)&ctl->status & kStatusStall);
@@ -1434,7 +1726,7 @@ __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_resident(Ctx c
 
 template <int ALG>
 __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_dispatch(Ctx c) {
-  __shared__ AnyShared sh;
+  __shared__ AnyShared<> sh;
   switch (c.ctl->variant) {  // same value for every thread of the launch
     case kVPThread: body_push<ALG, kVPThread>(c, sh.st); break;
     case kVPWarp: body_push<ALG, kVPWarp>(c, sh.st); break;

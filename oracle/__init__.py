@@ -27,7 +27,7 @@ _lib = None
 def build(ref: bool = True) -> None:
     """Build liboracle.so, and the _ref/ programs when the reference tree is present."""
     target = "all" if ref else "oracle"
-    subprocess.run(["make", "-s", "-C", str(HERE), target], check=True)
+    subprocess.run(["make", "-s", "-j", str(min(16, os.cpu_count() or 1)), "-C", str(HERE), target], check=True)
 
 
 def lib() -> C.CDLL:
@@ -248,6 +248,33 @@ def run_ref_program(name: str, args: list[str], threads: int | None = None, time
     tp = re.findall(r"Throughput:\s*([0-9.eE+-]+)\s*gigaedges/s", out)
     return {"rc": p.returncode, "out": out, "runtime": float(rt[-1]) if rt else None,
             "gteps": float(tp[-1]) if tp else None, "verified": "verification passed" in out}
+
+
+def bfs_programs() -> list[tuple[str, str]]:
+    """(model, program) of every reference OpenMP and C++-threads BFS program
+    built unchanged into _ref/bfs_omp and _ref/bfs_cpp."""
+    out = []
+    for model in ("omp", "cpp"):
+        d = REF_OUT / f"bfs_{model}"
+        if d.is_dir():
+            out += [(model, p.name) for p in sorted(d.iterdir()) if os.access(p, os.X_OK)]
+    return out
+
+
+def run_bfs_program(model: str, name: str, egr_path: str, src: int, threads: int, timeout: float = 600) -> dict:
+    """One run of a reference CPU BFS program through its own main(): the
+    median of its runs as it prints it, and its own verifier's verdict
+    (OpenMP programs take the thread count from OMP_NUM_THREADS, C++-threads
+    programs as an argument, include/bfs_vertex_cpp.h:91-110)."""
+    exe = REF_OUT / f"bfs_{model}" / name
+    args = [str(exe), egr_path, str(src), "1"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    if model == "cpp":
+        args += ["3", str(threads)]
+    p = subprocess.run(args, capture_output=True, text=True, env=env, timeout=timeout)
+    out = p.stdout + p.stderr
+    rt = re.findall(r"runtime:\s*([0-9.eE+-]+)\s*s", out)
+    return {"rc": p.returncode, "runtime": float(rt[-1]) if rt else None, "verified": "verification passed" in out}
 
 
 # ---------------------------------------------------------------------------

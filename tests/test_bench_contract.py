@@ -61,5 +61,5 @@ def test_reference_arm_line():
     import bench
 
     g = i2.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=22)
-    args = argparse.Namespace(variant="vp_cta", loop="graph", delta=0)
+    args = argparse.Namespace(variant="vp_cta", loop="graph", delta=0, budget=-1)
     assert d["config"] == bench.bench_config(args, g, 1)

@@ -265,6 +265,68 @@ def test_sssp_near_far_reduces_relaxed_work(gpu, seeded):
     dg.free()
 
 
+@pytest.mark.parametrize("name", ["er", "rmat14", "grid", "rmat16", "directed", "unit"])
+def test_sssp_budget_ordering_any_budget(gpu, seeded, name):
+    # The budgeted near/far ordering keeps each near frontier at about B edges:
+    # it trims large frontiers (the threshold falls), histograms the far pile
+    # when the frontier runs dry (the threshold rises) and drops pile entries a
+    # near push superseded. Distances must not depend on B, including B far
+    # below one vertex's degree and far above the graph, in every loop mode.
+    if name == "directed":
+        g = _directed_chain()
+    elif name == "unit":
+        g0 = seeded["rmat14"]
+        g = i2.ECLGraph(g0.nodes, g0.edges, g0.nindex, g0.nlist, np.ones(g0.edges, np.int32))
+    else:
+        g = seeded[name]
+    dg = i2.DeviceGraph.upload(g)
+    deg = g.degrees()
+    srcs = [0, int(np.argmax(deg))] if name != "directed" else [0, 4]
+    for s in srcs:
+        ref = oracle.sssp(g, s)
+        for budget in (1, 7, 100, 5000, 1 << 20, i2.I2_SSSP_BUDGET_AUTO):
+            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST, i2.I2_LOOP_RELAUNCH):
+                d, rep = dg.sssp(s, variant="vp_cta", loop=loop, budget=budget)
+                np.testing.assert_array_equal(d, ref, err_msg=f"{name} src {s} budget {budget} loop {loop}")
+                assert rep.reached_vertices == int((ref != i2.INF).sum())
+    dg.free()
+
+
+def test_sssp_budget_golden_repeat_and_step_precedence(gpu, golden):
+    # Piles, histograms and thresholds must not leak into the next run, and a
+    # fixed step (sssp_delta > 0) takes precedence over a budget.
+    for name, case in golden.items():
+        dg = i2.DeviceGraph.upload(case["graph"])
+        for s in case["sources"][:8]:
+            for budget, delta in ((3, 0), (64, 0), (i2.I2_SSSP_BUDGET_AUTO, 0), (3, 64)):
+                for _ in range(2):
+                    d, _ = dg.sssp(s, variant="vp_cta", delta=delta, budget=budget)
+                    np.testing.assert_array_equal(d, case["sssp"][s], err_msg=f"{name} {s} {budget} {delta}")
+        dg.free()
+
+
+def test_sssp_budget_reduces_relaxed_work(gpu, seeded):
+    # On a skewed graph from its hub, plain frontier-driven relaxation scans
+    # the reached edges more than twice; a budget of a few percent of the edges
+    # must cut the edges relaxed (relaxation launches only: trims and moves
+    # relax nothing) well below that, and the launch records must show the
+    # trims and moves that do it.
+    g = seeded["rmat16"]
+    dg = i2.DeviceGraph.upload(g)
+    src = int(np.argmax(g.degrees()))
+    _, rep0 = dg.sssp(src, variant="vp_cta", record=True)
+    plain = sum(r["edges"] for r in dg.records())
+    d, rep = dg.sssp(src, variant="vp_cta", budget=g.edges // 32, record=True)
+    np.testing.assert_array_equal(d, oracle.sssp(g, src))
+    recs = dg.records()
+    relaxed = sum(r["edges"] for r in recs if r["kind"] == 0)
+    kinds = {r["kind"] for r in recs}
+    assert {0, 1, 3} <= kinds, kinds
+    assert plain > 1.5 * rep0.reached_edges
+    assert relaxed < 0.75 * plain, (relaxed, plain, rep0.reached_edges)
+    dg.free()
+
+
 def test_union_find_cc(gpu, seeded, golden):
     # Union-find CC reaches the minimum-ID labels from the initial labels and,
     # switched to mid-traversal by a selector, from any label-propagation
