@@ -190,6 +190,30 @@ int i2_graph_wrap_device(const i2_eclgraph* dev, i2_graph** out);
 /* Generate an RMAT graph directly on the device (identical CSR to i2_gen_rmat). */
 int i2_graph_generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
                            int weighted, i2_graph** out);
+/* RMAT on n vertices directly on the device (identical CSR to i2_gen_rmat_n). */
+int i2_graph_generate_rmat_n(int n, int edge_factor, double a, double b, double c, uint64_t seed, int weighted,
+                             i2_graph** out);
+/* Generate G(n, m) directly on the device (identical CSR to i2_gen_er). */
+int i2_graph_generate_er(int n, long long m, uint64_t seed, int weighted, i2_graph** out);
+/* Generate the grid graph directly on the device (identical CSR to i2_gen_grid). */
+int i2_graph_generate_grid(int side, double remove_frac, double add_frac, uint64_t seed, int weighted,
+                           i2_graph** out);
+/* Build a CSR graph on the device from m directed pairs (src[k], dst[k]) and,
+   if w is not NULL, their int32 weights, all in device memory of the current
+   GPU (no counterpart in the reference, whose graphs come from .egr files;
+   the host analogue of its sp[] loop is include/bfs_edge_cuda.h:140-146).
+   symmetrize != 0 adds the reverse of every pair. Self-loops are dropped,
+   duplicate pairs merged (keeping the smallest weight), adjacency sorted.
+   Pairs outside [0, nodes) give I2_ERR_FORMAT. */
+int i2_graph_from_coo_device(int nodes, long long m, const int* src, const int* dst, const int* w,
+                             int symmetrize, i2_graph** out);
+/* The highest-degree vertex (lowest ID on ties), the benchmark configurations' source. */
+int i2_graph_hub(i2_graph* g, int* v);
+/* The starting-point array sp[e] = source vertex of CSR entry e (the
+   reference's host loop, include/bfs_edge_cuda.h:140-146), built on the device
+   on first need: *sp_dev receives its device address (valid while g lives),
+   and sp_host (edges ints, may be NULL) a copy. */
+int i2_graph_sp(i2_graph* g, const int** sp_dev, int* sp_host);
 int i2_graph_size(const i2_graph* g, int* nodes, int* edges);
 int i2_graph_degree(const i2_graph* g, int v, int* deg);
 /* Statistics of the graph; the first call also checks symmetry (one pass over the CSR). */
@@ -278,6 +302,9 @@ int i2_run_noalloc(int algo, const i2_eclgraph* dev, int src, int* dist_dev, voi
 /* ---- batches of graphs traversed together ---- */
 typedef struct i2_batch i2_batch;
 int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out);
+/* The same batch from graphs already on the device (copied device to device;
+   the graphs stay owned by the caller). */
+int i2_batch_from_device(i2_graph* const* graphs, int n, i2_batch** out);
 /* dist: host array of sum(nodes) ints, graph k's vertices at offset voff[k]. */
 int i2_batch_run(i2_batch* b, int algo, const int* srcs, int* dist, const i2_opts* opts, i2_report* rep);
 int i2_batch_offsets(const i2_batch* b, long long* voff);

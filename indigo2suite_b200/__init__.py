@@ -248,6 +248,56 @@ class DeviceGraph:
                "device rmat")
         return cls(h)
 
+    @classmethod
+    def generate_rmat_n(cls, n: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                        seed: int = 1, weighted: bool = True) -> "DeviceGraph":
+        """RMAT on n vertices built on the device: the same CSR as gen_rmat_n."""
+        h = C.c_void_p()
+        _check(lib.i2_graph_generate_rmat_n(n, edge_factor, a, b, c, seed, int(weighted), C.byref(h)),
+               "device rmat_n")
+        return cls(h)
+
+    @classmethod
+    def generate_er(cls, n: int, m: int, seed: int = 1, weighted: bool = True) -> "DeviceGraph":
+        """G(n, m) built on the device: the same CSR as gen_er."""
+        h = C.c_void_p()
+        _check(lib.i2_graph_generate_er(n, m, seed, int(weighted), C.byref(h)), "device er")
+        return cls(h)
+
+    @classmethod
+    def generate_grid(cls, side: int, remove_frac: float = 0.05, add_frac: float = 0.001, seed: int = 1,
+                      weighted: bool = True) -> "DeviceGraph":
+        """The grid graph built on the device: the same CSR as gen_grid."""
+        h = C.c_void_p()
+        _check(lib.i2_graph_generate_grid(side, remove_frac, add_frac, seed, int(weighted), C.byref(h)),
+               "device grid")
+        return cls(h)
+
+    @classmethod
+    def from_coo_device(cls, nodes: int, m: int, src_ptr: int, dst_ptr: int, w_ptr: int = 0,
+                        symmetrize: bool = False) -> "DeviceGraph":
+        """CSR built on the device from m (src, dst[, w]) pairs already in device
+        memory (e.g. torch tensors' data_ptr()): self-loops dropped, duplicates
+        merged keeping the smallest weight, adjacency sorted."""
+        h = C.c_void_p()
+        _check(lib.i2_graph_from_coo_device(nodes, m, C.c_void_p(src_ptr), C.c_void_p(dst_ptr),
+                                            C.c_void_p(w_ptr) if w_ptr else None, int(symmetrize), C.byref(h)),
+               "coo to csr")
+        return cls(h)
+
+    def hub(self) -> int:
+        """The highest-degree vertex (lowest ID on ties)."""
+        v = C.c_int()
+        _check(lib.i2_graph_hub(self._h, C.byref(v)), "hub")
+        return v.value
+
+    def sp(self) -> np.ndarray:
+        """The starting-point array sp[e] (source vertex of CSR entry e), built on the device."""
+        out = np.empty(max(1, self.edges), np.int32)
+        dp = C.c_void_p()
+        _check(lib.i2_graph_sp(self._h, C.byref(dp), _iptr(out)), "sp")
+        return out[: self.edges]
+
     def download(self) -> ECLGraph:
         cg = capi.EclGraphC()
         _check(lib.i2_graph_download(self._h, C.byref(cg)), "graph download")
@@ -343,13 +393,19 @@ def _rec(r: capi.IterRecord) -> dict:
 
 
 class Batch:
-    """Many graphs traversed together as one disjoint-union CSR."""
+    """Many graphs traversed together as one disjoint-union CSR: from host
+    graphs (ECLGraph, uploaded) or from device graphs (DeviceGraph, copied on
+    the device)."""
 
-    def __init__(self, graphs: list[ECLGraph]):
+    def __init__(self, graphs: list):
         self.graphs = graphs
-        arr = (capi.EclGraphC * len(graphs))(*[g.as_c() for g in graphs])
         self._h = C.c_void_p()
-        _check(lib.i2_batch_upload(arr, len(graphs), C.byref(self._h)), "batch upload")
+        if graphs and isinstance(graphs[0], DeviceGraph):
+            arr = (C.c_void_p * len(graphs))(*[g._h for g in graphs])
+            _check(lib.i2_batch_from_device(arr, len(graphs), C.byref(self._h)), "batch from device")
+        else:
+            arr = (capi.EclGraphC * len(graphs))(*[g.as_c() for g in graphs])
+            _check(lib.i2_batch_upload(arr, len(graphs), C.byref(self._h)), "batch upload")
         voff = (C.c_longlong * (len(graphs) + 1))()
         _check(lib.i2_batch_offsets(self._h, voff), "batch offsets")
         self.voff = np.array(list(voff), np.int64)

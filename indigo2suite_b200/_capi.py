@@ -93,6 +93,15 @@ SIGNATURES = {
     "i2_gen_grid": (_I, [_I, C.c_double, C.c_double, C.c_uint64, _I, _PG]),
     "i2_graph_upload": (_I, [_PG, C.POINTER(_P)]),
     "i2_graph_wrap_device": (_I, [_PG, C.POINTER(_P)]),
+    "i2_graph_generate_rmat_n": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I,
+                                      C.POINTER(C.c_void_p)]),
+    "i2_batch_from_device": (_I, [C.POINTER(C.c_void_p), _I, C.POINTER(C.c_void_p)]),
+    "i2_graph_generate_er": (_I, [_I, C.c_longlong, C.c_uint64, _I, C.POINTER(C.c_void_p)]),
+    "i2_graph_generate_grid": (_I, [_I, C.c_double, C.c_double, C.c_uint64, _I, C.POINTER(C.c_void_p)]),
+    "i2_graph_from_coo_device": (_I, [_I, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, _I,
+                                      C.POINTER(C.c_void_p)]),
+    "i2_graph_sp": (_I, [C.c_void_p, C.POINTER(C.c_void_p), _PI]),
+    "i2_graph_hub": (_I, [C.c_void_p, _PI]),
     "i2_graph_generate_rmat": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I,
                                     C.POINTER(_P)]),
     "i2_graph_size": (_I, [_P, _PI, _PI]),

@@ -21,6 +21,13 @@ __global__ void k_shift(int* a, long long n, int delta) {
   for (long long k = tid; k < n; k += stride) a[k] += delta;
 }
 
+// dst[k] = src[k] + delta (device to device, one graph of a batch).
+__global__ void k_copy_shift(int* __restrict__ dst, const int* __restrict__ src, long long n, int delta) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = tid; k < n; k += stride) dst[k] = src[k] + delta;
+}
+
 }  // namespace i2
 
 using namespace i2;
@@ -55,15 +62,19 @@ int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out) {
   if (e == cudaSuccess && weighted) e = dev_alloc(&w, sizeof(int) * (E + 4));
   i2_batch* b = new i2_batch();
   b->n = n;
+  // Entry ranges must be valid before anything indexes through them (all
+  // graphs checked in parallel).
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+  for (int k = 0; k < n; ++k) {
+    const i2_eclgraph& h = graphs[k];
+    for (long long x = 0; x < h.edges; ++x) bad |= (unsigned)h.nlist[x] >= (unsigned)h.nodes;
+    for (int v = 0; v < h.nodes; ++v) bad |= h.nindex[v + 1] < h.nindex[v];
+  }
+  if (bad) e = cudaErrorInvalidValue;
   long long vo = 0, eo = 0;
   for (int k = 0; k < n && e == cudaSuccess; ++k) {
     const i2_eclgraph& h = graphs[k];
-    // Entry ranges must be valid before anything indexes through them.
-    for (long long x = 0; x < h.edges; ++x)
-      if ((unsigned)h.nlist[x] >= (unsigned)h.nodes) e = cudaErrorInvalidValue;
-    for (int v = 0; v < h.nodes && e == cudaSuccess; ++v)
-      if (h.nindex[v + 1] < h.nindex[v]) e = cudaErrorInvalidValue;
-    if (e != cudaSuccess) break;
     b->voff.push_back(vo);
     b->eoff.push_back(eo);
     e = cudaMemcpy(nindex + vo, h.nindex, sizeof(int) * h.nodes, cudaMemcpyHostToDevice);
@@ -88,6 +99,59 @@ int i2_batch_upload(const i2_eclgraph* graphs, int n, i2_batch** out) {
     dev_free(w);
     delete b;
     return bad_input ? I2_ERR_FORMAT : cuda_status(e);
+  }
+  int st = graph_adopt((int)V, (int)E, nindex, nlist, w, &b->g);
+  if (st) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return I2_OK;
+}
+
+int i2_batch_from_device(i2_graph* const* graphs, int n, i2_batch** out) {
+  if (!graphs || n < 1 || !out) return I2_ERR_ARG;
+  *out = nullptr;
+  std::vector<int> nv(n), ne(n);
+  std::vector<const int*> ni(n), nl(n), nw(n);
+  long long V = 0, E = 0;
+  int weighted = 1;
+  for (int k = 0; k < n; ++k) {
+    if (!graphs[k] || graph_device_csr(graphs[k], &nv[k], &ne[k], &ni[k], &nl[k], &nw[k])) return I2_ERR_ARG;
+    V += nv[k];
+    E += ne[k];
+    if (!nw[k]) weighted = 0;
+  }
+  if (V > 0x7ffffffeLL || E > 0x7ffffffbLL) return I2_ERR_OVERFLOW;
+  int *nindex = nullptr, *nlist = nullptr, *w = nullptr;
+  cudaError_t e = dev_alloc(&nindex, sizeof(int) * (V + 1));
+  if (e == cudaSuccess) e = dev_alloc(&nlist, sizeof(int) * (E + 4));
+  if (e == cudaSuccess && weighted) e = dev_alloc(&w, sizeof(int) * (E + 4));
+  i2_batch* b = new i2_batch();
+  b->n = n;
+  long long vo = 0, eo = 0;
+  for (int k = 0; k < n && e == cudaSuccess; ++k) {
+    b->voff.push_back(vo);
+    b->eoff.push_back(eo);
+    // each graph's arrays were validated when it was built or uploaded
+    k_copy_shift<<<256, 256>>>(nindex + vo, ni[k], nv[k], (int)eo);
+    if (ne[k]) k_copy_shift<<<1024, 256>>>(nlist + eo, nl[k], ne[k], (int)vo);
+    if (weighted && ne[k]) e = cudaMemcpyAsync(w + eo, nw[k], sizeof(int) * ne[k], cudaMemcpyDeviceToDevice);
+    vo += nv[k];
+    eo += ne[k];
+  }
+  if (e == cudaSuccess) {
+    const int Ei = (int)E;
+    e = cudaMemcpy(nindex + V, &Ei, sizeof(int), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    dev_free(nindex);
+    dev_free(nlist);
+    dev_free(w);
+    delete b;
+    return cuda_status(e);
   }
   int st = graph_adopt((int)V, (int)E, nindex, nlist, w, &b->g);
   if (st) {

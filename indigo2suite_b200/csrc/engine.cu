@@ -150,6 +150,20 @@ __global__ void k_reset(Ctl* ctl, RunParams p) {
 // ---------------------------------------------------------------------------
 // Graph maintenance kernels.
 
+// *best = the smallest vertex of degree maxdeg.
+__global__ void k_hub(DGraph g, int maxdeg, int* best) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int b = INT_MAX;
+  for (long long v = tid; v < g.nodes; v += stride)
+    if (g.nindex[v + 1] - g.nindex[v] == maxdeg) {
+      b = (int)v;
+      break;  // later vertices of this thread are larger
+    }
+  for (int o = 16; o > 0; o >>= 1) b = min(b, __shfl_down_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0 && b != INT_MAX) atomicMin(best, b);
+}
+
 // Sets bit 8 of *bad when a weight is negative (SSSP needs weights >= 0).
 __global__ void k_negative_weights(const int* w, long long n, int* bad) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1222,6 +1236,58 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
   return I2_OK;
 }
 
+// True when [p, p + bytes) lies inside one device (or managed) allocation of
+// the current context. Host pointers, pinned or not, are refused: a kernel
+// given one would fault or read the wrong memory. So is device memory of
+// another GPU: kernels launched on the current device would read it through a
+// peer mapping, or fault where there is none.
+typedef int (*MemGetAddressRangeFn)(unsigned long long*, size_t*, unsigned long long);
+
+int graph_device_csr(const i2_graph* g, int* nodes, int* edges, const int** nindex, const int** nlist,
+                     const int** eweight) {
+  if (!g) return I2_ERR_ARG;
+  *nodes = g->g.nodes;
+  *edges = g->g.edges;
+  *nindex = g->g.nindex;
+  *nlist = g->g.nlist;
+  *eweight = g->g.eweight;
+  return I2_OK;
+}
+
+bool device_range_ok(const void* p, size_t bytes) {
+  if (bytes == 0) return true;
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+  if (a.type == cudaMemoryTypeDevice) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || a.device != cur) {
+      cudaGetLastError();
+      return false;
+    }
+  }
+  static MemGetAddressRangeFn range_fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range_fn = (MemGetAddressRangeFn)fn;
+    cudaGetLastError();
+  }
+  if (!range_fn) return true;  // type check only
+  unsigned long long base = 0;
+  size_t size = 0;
+  if (range_fn(&base, &size, (unsigned long long)(uintptr_t)p) != 0) return false;
+  return (unsigned long long)(uintptr_t)p + bytes <= base + size;
+}
+
 }  // namespace i2
 
 // ---------------------------------------------------------------------------
@@ -1332,45 +1398,33 @@ int i2_graph_upload(const i2_eclgraph* h, i2_graph** out) {
   return I2_OK;
 }
 
-// True when [p, p + bytes) lies inside one device (or managed) allocation of
-// the current context. Host pointers, pinned or not, are refused: a kernel
-// given one would fault or read the wrong memory. So is device memory of
-// another GPU: kernels launched on the current device would read it through a
-// peer mapping, or fault where there is none.
-typedef int (*MemGetAddressRangeFn)(unsigned long long*, size_t*, unsigned long long);
+int i2_graph_hub(i2_graph* g, int* v) {
+  if (!g || !v) return I2_ERR_ARG;
+  I2_CK(cudaSetDevice(g->device));
+  int* d = nullptr;
+  I2_CK(dev_alloc(&d, sizeof(int)));
+  int h = INT_MAX;
+  cudaError_t e = cudaMemcpyAsync(d, &h, sizeof(int), cudaMemcpyHostToDevice, g->stream);
+  if (e == cudaSuccess) {
+    k_hub<<<4 * sm_count(), 256, 0, g->stream>>>(g->g, g->gs.maxdeg, d);
+    e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, g->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  dev_free(d);
+  if (e != cudaSuccess) return cuda_status(e);
+  *v = h == INT_MAX ? 0 : h;
+  return I2_OK;
+}
 
-static bool device_range_ok(const void* p, size_t bytes) {
-  if (bytes == 0) return true;
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
-  if (a.type == cudaMemoryTypeDevice) {
-    int cur = -1;
-    if (cudaGetDevice(&cur) != cudaSuccess || a.device != cur) {
-      cudaGetLastError();
-      return false;
-    }
-  }
-  static MemGetAddressRangeFn range_fn = nullptr;
-  static bool looked = false;
-  if (!looked) {
-    looked = true;
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      range_fn = (MemGetAddressRangeFn)fn;
-    cudaGetLastError();
-  }
-  if (!range_fn) return true;  // type check only
-  unsigned long long base = 0;
-  size_t size = 0;
-  if (range_fn(&base, &size, (unsigned long long)(uintptr_t)p) != 0) return false;
-  return (unsigned long long)(uintptr_t)p + bytes <= base + size;
+int i2_graph_sp(i2_graph* g, const int** sp_dev, int* sp_host) {
+  if (!g || (!sp_dev && !sp_host)) return I2_ERR_ARG;
+  I2_CK(cudaSetDevice(g->device));
+  int st = ensure_sp(g);
+  if (st) return st;
+  if (sp_dev) *sp_dev = g->d_sp;
+  if (sp_host && g->g.edges > 0)
+    I2_CK(cudaMemcpy(sp_host, g->d_sp, sizeof(int) * (size_t)g->g.edges, cudaMemcpyDeviceToHost));
+  return I2_OK;
 }
 
 int i2_graph_wrap_device(const i2_eclgraph* d, i2_graph** out) {

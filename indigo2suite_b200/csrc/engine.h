@@ -23,8 +23,16 @@ int mlp_install(const float* params, int count);
 int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
                   i2_report* rep);
 
+// True when [p, p + bytes) lies inside one allocation of the current device
+// (or managed memory); host pointers and other GPUs' memory are refused.
+bool device_range_ok(const void* p, size_t bytes);
+
 // Take ownership of CSR arrays already on the device and build a graph handle.
 int graph_adopt(int nodes, int edges, int* d_nindex, int* d_nlist, int* d_eweight, i2_graph** out);
+
+// The device CSR arrays of a graph (weights null when it has none).
+int graph_device_csr(const i2_graph* g, int* nodes, int* edges, const int** nindex, const int** nlist,
+                     const int** eweight);
 
 // Copy the last traversal's values to a host array of g.nodes ints.
 int graph_copy_result(i2_graph* g, int* host_out, const i2_opts* opts);

@@ -24,10 +24,9 @@ constexpr int kOffB3 = kOffW3 + kHidden * kOut;
 constexpr int kParams = kOffB3 + kOut;
 
 // Features of a frontier about to be consumed. All are finite and O(1..30).
-// The graph-size features and the iteration index are clamped to the range the
-// selector is trained on (graphs of 2^16..2^20 vertices, frontiers reaching
-// their steady state within 64 iterations), so that bigger graphs and long
-// tails are treated like the largest trained ones instead of extrapolated.
+// The graph-size features are clamped to 2^16..2^26 vertices and 2^17..2^31
+// CSR entries (the range from the training graphs to RMAT-26), and the
+// iteration index to 64 (frontiers reach their steady state by then).
 __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, int iter, int size, int hsize,
                                                   unsigned long long edges, int maxdeg, long long visited,
                                                   float* f) {
@@ -43,8 +42,8 @@ __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, in
   f[5] = log2f(1.f + (float)maxdeg);
   f[6] = (float)visited / V;
   f[7] = log2f(1.f + fminf((float)iter, 64.f));
-  f[8] = fminf(fmaxf(log2f(V), 16.f), 20.f);
-  f[9] = fminf(fmaxf(log2f(1.f + (float)gs.edges), 17.f), 25.f);
+  f[8] = fminf(fmaxf(log2f(V), 16.f), 26.f);
+  f[9] = fminf(fmaxf(log2f(1.f + (float)gs.edges), 17.f), 31.f);
   f[10] = log2f(1.f + gs.avgdeg);
   f[11] = log2f(1.f + (float)gs.maxdeg);
   f[12] = log2f(1.f + gs.degcv);

@@ -12,7 +12,9 @@ picks the next iteration's style on the device, without a host round trip.
 Every style reaches the same fixed point, so the selector changes time only.
 
 Usage:
-    python -m indigo2suite_b200.selector train [--graphs 200] [--out PATH]
+    python -m indigo2suite_b200.selector train [--graphs 200] [--max-scale 21] [--out PATH]
+        (also writes PATH with the suffix .json: the command, the sweep's and
+        the parameters' SHA-256, the row count and the final loss)
     python -m indigo2suite_b200.selector eval [--params PATH] [--json OUT]
 """
 from __future__ import annotations
@@ -55,11 +57,11 @@ class GraphSpec:
         return gen_grid(side, 0.05, 0.001, seed=self.seed)
 
 
-def training_specs(count: int = 200, seed: int = 2024) -> list[GraphSpec]:
-    """`count` seeded graphs, families RMAT/ER/grid in turn, scales 16..20."""
+def training_specs(count: int = 200, seed: int = 2024, max_scale: int = 21) -> list[GraphSpec]:
+    """`count` seeded graphs, families RMAT/ER/grid in turn, scales 16..max_scale."""
     rng = np.random.default_rng(seed)
     fams = ("rmat", "er", "grid")
-    return [GraphSpec(fams[k % 3], 16 + int(rng.integers(0, 5)), int(rng.integers(1, 2**31 - 1)))
+    return [GraphSpec(fams[k % 3], 16 + int(rng.integers(0, max_scale - 15)), int(rng.integers(1, 2**31 - 1)))
             for k in range(count)]
 
 
@@ -210,6 +212,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("cmd", choices=["train", "eval"])
     ap.add_argument("--graphs", type=int, default=200)
+    ap.add_argument("--max-scale", type=int, default=21)
     ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--out", default=str(PARAMS_PATH))
     ap.add_argument("--params", default=str(PARAMS_PATH))
@@ -221,12 +224,20 @@ def main(argv=None):
             z = np.load(a.data)
             X, T, M = z["X"], z["T"], z["M"]
         else:
-            X, T, M, _ = record(training_specs(a.graphs))
+            X, T, M, _ = record(training_specs(a.graphs, max_scale=a.max_scale))
             if a.data:
                 np.savez_compressed(a.data, X=X, T=T, M=M)
         p, loss = train(X, T, M, epochs=a.epochs)
         p.astype(np.float32).tofile(a.out)
-        print(json.dumps({"rows": int(X.shape[0]), "final_loss": loss, "out": a.out}))
+        import hashlib
+
+        digest = hashlib.sha256(X.tobytes() + T.tobytes() + M.tobytes()).hexdigest()
+        meta = {"command": f"python -m indigo2suite_b200.selector train --graphs {a.graphs} "
+                           f"--max-scale {a.max_scale} --epochs {a.epochs}",
+                "rows": int(X.shape[0]), "final_loss": loss, "sweep_sha256": digest,
+                "params_sha256": hashlib.sha256(p.astype(np.float32).tobytes()).hexdigest(), "out": a.out}
+        Path(a.out).with_suffix(".json").write_text(json.dumps(meta, indent=1) + "\n")
+        print(json.dumps(meta))
     else:
         p = np.fromfile(a.params, np.float32)
         rows = evaluate(p, eval_specs())

@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-from . import gen_er, gen_grid, gen_rmat_n
+from . import DeviceGraph, gen_er, gen_grid, gen_rmat_n
 
 
 def batch_specs(count: int = 512, seed: int = 4, nmin: float = 1e3, nmax: float = 1e6):
@@ -38,6 +38,17 @@ def build(spec):
         return gen_rmat_n(n, 16, 0.57, 0.19, 0.19, seed=seed)
     side = int(math.ceil(math.sqrt(n)))
     return gen_grid(side, 0.05, 0.001, seed=seed)
+
+
+def build_device(spec) -> DeviceGraph:
+    """The same graph as build(spec), generated on the device."""
+    fam, n, seed = spec
+    if fam == "er":
+        return DeviceGraph.generate_er(n, 4 * n, seed)
+    if fam == "rmat":
+        return DeviceGraph.generate_rmat_n(n, 16, 0.57, 0.19, 0.19, seed=seed)
+    side = int(math.ceil(math.sqrt(n)))
+    return DeviceGraph.generate_grid(side, 0.05, 0.001, seed=seed)
 
 
 def source(g) -> int:
