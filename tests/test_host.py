@@ -189,3 +189,58 @@ def test_noalloc_argument_checks_come_before_any_device_work():
     assert i2.lib.i2_run_noalloc(i2.I2_SSSP, C.byref(g), 0, out, None, None) == _capi.I2_ERR_ARG  # no weights
     big = _capi.EclGraphC((1 << 17) + 1, 0, C.cast(C.c_void_p(0x1000), P), P(), P())
     assert i2.lib.i2_run_noalloc(i2.I2_BFS, C.byref(big), 0, out, None, None) == _capi.I2_ERR_CAPACITY
+
+
+def test_traversal_tuning_table_lookup(tmp_path):
+    """Single traversals are tuned by shape: degree class and nearest size
+    class of the same algorithm; unknown shapes keep the defaults."""
+    import json
+
+    from indigo2suite_b200 import autotune
+
+    assert autotune.degree_class({"degcv": 3.0, "avgdeg": 30.0}) == "skewed"
+    assert autotune.degree_class({"degcv": 0.3, "avgdeg": 8.0}) == "uniform"
+    assert autotune.degree_class({"degcv": 0.2, "avgdeg": 3.8}) == "sparse"
+    assert autotune.size_class(1 << 22) == 22 and autotune.size_class(3_000_000) == 22
+    assert autotune.size_class(1 << 19) in (18, 20)
+    assert {b for _, b in autotune.traversal_candidates("sssp")} == set(autotune.TUNE_BUDGETS)
+    assert {b for _, b in autotune.traversal_candidates("bfs")} == {0}
+    t = {"rows": [{"graph": "rmat18", "class": "skewed", "log2v": 18, "algo": "sssp", "blocks_per_sm": 4,
+                   "budget": 1 << 20},
+                  {"graph": "rmat22", "class": "skewed", "log2v": 22, "algo": "sssp", "blocks_per_sm": 8,
+                   "budget": 1 << 22}]}
+    p = tmp_path / "t.json"
+    p.write_text(json.dumps(t))
+    info = {"degcv": 4.0, "avgdeg": 30.0, "nodes": 1 << 21}
+    assert autotune.lookup(info, "sssp", p)["budget"] == 1 << 22  # size 22 is the nearest class
+    assert autotune.lookup(dict(info, nodes=1 << 17), "sssp", p)["budget"] == 1 << 20
+    assert autotune.lookup(dict(info, degcv=0.1), "sssp", p) is None
+    assert autotune.lookup(info, "bfs", p) is None
+    assert autotune.lookup(info, "sssp", tmp_path / "missing.json") is None
+    if autotune.TRAVERSAL_TABLE.exists():
+        table = json.loads(autotune.TRAVERSAL_TABLE.read_text())
+        assert len(table["rows"]) > 1
+        for r in table["rows"]:  # every committed choice is its row's fastest candidate
+            best = min(r["candidates"], key=lambda c: c["ms"])
+            assert (best["blocks_per_sm"], best["budget"]) == (r["blocks_per_sm"], r["budget"])
+        # and it measurably beats the default on at least one shape
+        assert any(r["ms"] < 0.9 * r["default_ms"] for r in table["rows"])
+
+
+def test_selector_parameters_match_their_recorded_training():
+    """The committed parameters name the command and sweep that made them, and
+    the committed sweep is the one whose hash they record."""
+    import hashlib
+    import json
+
+    from indigo2suite_b200 import selector as S
+
+    meta = json.loads(S.PARAMS_PATH.with_suffix(".json").read_text())
+    p = np.fromfile(S.PARAMS_PATH, np.float32)
+    assert p.size == i2.mlp_param_count()
+    assert hashlib.sha256(p.tobytes()).hexdigest() == meta["params_sha256"]
+    z = np.load(S.PARAMS_PATH.with_name("selector_sweep.npz"))
+    assert z["X"].shape == (meta["rows"], 16)
+    h = hashlib.sha256(z["X"].tobytes() + z["T"].tobytes() + z["M"].tobytes()).hexdigest()
+    assert h == meta["sweep_sha256"]
+    assert "selector train" in meta["command"] and "--data" in meta["command"]

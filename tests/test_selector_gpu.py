@@ -1,7 +1,14 @@
 """The learned style selector (committed parameters) on graphs it was not
-trained on: it never changes a result, and on high-diameter graphs it takes
-the pull and topology styles that the fixed frontier-size heuristic never
-picks there, without losing much time against it."""
+trained on (the held-out set of `selector.eval_specs()`, fixed before
+training: RMAT / ER / grid of 2^18 and 2^20 vertices, seeds 7000-7005).
+
+* It never changes a result.
+* Against the frontier-size rule it falls back to (the heuristic), it is not
+  slower overall: median of 7 resident traversals per case, BFS / SSSP / CC.
+* Where the network overrides the rule (styles the rule never picks, such as
+  the topology-driven pull on grids), it is faster: that is what the trained
+  network adds to the method without it.
+"""
 import math
 
 import numpy as np
@@ -13,6 +20,8 @@ from indigo2suite_b200 import selector as S
 
 pytestmark = pytest.mark.gpu
 
+RULE_STYLES = {i2.VARIANTS.index(v) for v in ("vp_thread", "vp_cta", "pull_frontier", "union_find")}
+
 
 @pytest.fixture(scope="module")
 def params(gpu):
@@ -22,9 +31,13 @@ def params(gpu):
     return p
 
 
-def _median_ms(dg, algo, src, variant, runs=5):
+def _median_ms(dg, algo, src, variant, runs=7):
     dg.run_device(algo, src, variant=variant)
     return sorted(dg.run_device(algo, src, variant=variant).seconds for _ in range(runs))[runs // 2] * 1e3
+
+
+def _geo(xs):
+    return math.exp(sum(math.log(x) for x in xs) / len(xs))
 
 
 def test_learned_results_are_bit_exact(params):
@@ -39,26 +52,19 @@ def test_learned_results_are_bit_exact(params):
         dg.free()
 
 
-def test_learned_moves_grid_iterations_to_pull_styles(params):
-    # What the trained network adds over the fixed rule on high-diameter
-    # graphs: it moves BFS and SSSP iterations from the push to the pull and
-    # topology styles, which the rule never picks on grids. Its time against
-    # the rule's on held-out grids of 2^18 and 2^20 vertices measured
-    # 0.89-1.07x, depending on the box and the build (the push has become
-    # faster since the network was trained), so of the time only "not much
-    # slower" is asserted.
-    pull = {i2.VARIANTS.index("pull_frontier"), i2.VARIANTS.index("pull_topo")}
-    ratios = []
-    for spec in (S.GraphSpec("grid", 18, 8104), S.GraphSpec("grid", 18, 8106), S.GraphSpec("grid", 20, 8105)):
+def test_learned_not_slower_than_rule_and_faster_where_it_overrides(params):
+    ratios, overridden = [], []
+    for spec in S.eval_specs():
         g = spec.build()
         dg = i2.DeviceGraph.upload(g)
         src = int(np.argmax(g.degrees()))
-        for algo in (i2.I2_BFS, i2.I2_SSSP):
-            _, rl = dg._run(algo, src, "learned", i2.I2_LOOP_GRAPH, 0, False, None, None)
-            _, rh = dg._run(algo, src, "heuristic", i2.I2_LOOP_GRAPH, 0, False, None, None)
-            assert sum(rl.variant_hist[k] for k in pull) > 0.2 * rl.iterations, (spec, algo, rl.variant_hist)
-            assert sum(rh.variant_hist[k] for k in pull) == 0, (spec, algo, rh.variant_hist)
-            ratios.append(_median_ms(dg, algo, src, "learned", 7) / _median_ms(dg, algo, src, "heuristic", 7))
+        for algo in (i2.I2_BFS, i2.I2_SSSP, i2.I2_CC):
+            _, rep = dg._run(algo, src, "learned", i2.I2_LOOP_GRAPH, 0, False, None)
+            r = _median_ms(dg, algo, src, "learned") / _median_ms(dg, algo, src, "heuristic")
+            ratios.append(r)
+            if any(n and k not in RULE_STYLES for k, n in enumerate(rep.variant_hist)):
+                overridden.append(r)
         dg.free()
-    geo = math.exp(sum(math.log(r) for r in ratios) / len(ratios))
-    assert geo < 1.15, ratios
+    assert _geo(ratios) <= 1.03, ratios
+    assert len(overridden) >= 3, ratios
+    assert _geo(overridden) < 1.0, overridden
