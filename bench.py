@@ -700,9 +700,10 @@ def run_grid4096(args, rank: int, world: int, local: int):
 
 
 def run_rmat26(args, rank: int, world: int, local: int):
-    """Config: RMAT scale 26, 64 seeded sources (degree >= 1) for BFS and SSSP,
-    CC once; learned selector vs the edge-balanced fixed style. Sources shard
-    across ranks."""
+    """Config: RMAT scale 26 (--scale), 64 seeded sources (--sources; degree
+    >= 1) for BFS and SSSP, CC once; the edge-balanced fixed style (SSSP also
+    with the budgeted near/far ordering), the heuristic and the learned
+    selector. Sources shard across ranks."""
     import torch
 
     import indigo2suite_b200 as i2
@@ -714,17 +715,19 @@ def run_rmat26(args, rank: int, world: int, local: int):
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
     t0 = time.time()
-    dg = i2.DeviceGraph.generate_rmat(26, 16, 0.57, 0.19, 0.19, seed=26)
+    loop = {"graph": i2.I2_LOOP_GRAPH, "host": i2.I2_LOOP_HOST, "relaunch": i2.I2_LOOP_RELAUNCH}[args.loop]
+    nsrc = args.sources
+    dg = i2.DeviceGraph.generate_rmat(args.scale, 16, 0.57, 0.19, 0.19, seed=args.scale)
     gen_s = time.time() - t0
     if SELECTOR_PARAMS.exists():
         i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
-    rng = np.random.default_rng(26)
+    rng = np.random.default_rng(args.scale)
     srcs = []
-    while len(srcs) < 64:
+    while len(srcs) < nsrc:
         v = int(rng.integers(0, dg.nodes))
         if dg.degree(v) > 0:
             srcs.append(v)
-    lo, hi = shard.shard_range(64, rank, world)
+    lo, hi = shard.shard_range(nsrc, rank, world)
     mine = srcs[lo:hi]
     res = {}
     peak, peak_kind = peaks()
@@ -737,17 +740,21 @@ def run_rmat26(args, rank: int, world: int, local: int):
         b_alg = {"bfs": 8.0 * rep.reached_edges + 20.0 * rep.reached_vertices,
                  "sssp": 12.0 * rep.reached_edges + 20.0 * rep.reached_vertices,
                  "cc": 8.0 * dg.edges + 12.0 * dg.nodes}[an]
-        for v in ("vp_cta", "heuristic", "learned"):
+        rows = [("vp_cta", "vp_cta", 0), ("heuristic", "heuristic", 0), ("learned", "learned", 0)]
+        if algo == i2.I2_SSSP:
+            rows.insert(1, ("vp_cta_budget", "vp_cta", i2.I2_SSSP_BUDGET_AUTO))
+        for name, v, budget in rows:
             ss = mine if algo != i2.I2_CC else mine[:1]
-            dg.run_device(algo, ss[0], variant=v, stream=sp, report=False)
+            run = lambda s_: dg.run_device(algo, s_, variant=v, loop=loop, stream=sp, report=False,
+                                           budget=budget)
+            run(ss[0])
             torch.cuda.synchronize()
             it = iter(ss)
-            t = _event_time(torch, stream, lambda: dg.run_device(algo, next(it), variant=v, stream=sp, report=False),
-                            len(ss))
+            t = _event_time(torch, stream, lambda: run(next(it)), len(ss))
             t = dist.max(t, dev)
-            res[f"{an}/{v}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t,
-                                "b_alg_gb": 1e-9 * b_alg, "achieved_gbs": 1e-9 * b_alg / t,
-                                "roofline_frac": 1e-9 * b_alg / t / peak}
+            res[f"{an}/{name}"] = {"ms_per_traversal": 1e3 * t, "gteps": 1e-9 * dg.edges / t,
+                                   "b_alg_gb": 1e-9 * b_alg, "achieved_gbs": 1e-9 * b_alg / t,
+                                   "roofline_frac": 1e-9 * b_alg / t / peak}
     clk = clocks.stop()
     # results of the measured configurations from two of this rank's sources,
     # checked by the size-independent certificates (no serial run over 2e9 edges)
@@ -758,23 +765,29 @@ def run_rmat26(args, rank: int, world: int, local: int):
     for s_ in mine[:2]:
         for v in ("vp_cta", "heuristic", "learned"):
             for an, algo, wt in (("bfs", i2.I2_BFS, False), ("sssp", i2.I2_SSSP, True)):
-                d = dg._run(algo, s_, v, i2.I2_LOOP_GRAPH, 0, False, None)[0]
+                d = dg._run(algo, s_, v, loop, 0, False, None)[0]
                 c = oracle.certify_distances(host, s_, d, weighted=wt)
                 if c is not None:
                     raise SystemExit(f"rmat26 {an} {v} source {s_}: certificate failed: {c}")
                 verified[f"{an}/{v}/src{s_}"] = "shortest-path certificate"
+        d = dg._run(i2.I2_SSSP, s_, "vp_cta", loop, 0, False, None, budget=i2.I2_SSSP_BUDGET_AUTO)[0]
+        c = oracle.certify_distances(host, s_, d, weighted=True)
+        if c is not None:
+            raise SystemExit(f"rmat26 sssp vp_cta_budget source {s_}: certificate failed: {c}")
+        verified[f"sssp/vp_cta_budget/src{s_}"] = "shortest-path certificate"
     for v in ("vp_cta", "heuristic", "learned"):
-        lab = dg._run(i2.I2_CC, 0, v, i2.I2_LOOP_GRAPH, 0, False, None)[0]
+        lab = dg._run(i2.I2_CC, 0, v, loop, 0, False, None)[0]
         c = oracle.certify_cc(host, lab)
         if c is not None:
             raise SystemExit(f"rmat26 cc {v}: certificate failed: {c}")
         verified[f"cc/{v}"] = "minimum-label certificate"
     del host
     line = {"metric": METRIC, "value": world * res["bfs/learned"]["gteps"], "unit": UNIT, "n_gpus": world,
-            "steps": 64, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "steps": nsrc, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
-            "config": {"workload": "rmat26_bfs_sssp_cc_64src", "nodes": dg.nodes, "edges": dg.edges,
-                       "generation_s": gen_s, "parallelism": f"sources sharded x{world}"},
+            "config": {"workload": f"rmat{args.scale}_bfs_sssp_cc_{nsrc}src", "nodes": dg.nodes,
+                       "edges": dg.edges, "generation_s": gen_s, "loop": args.loop,
+                       "parallelism": f"sources sharded x{world}"},
             "roofline_peak_gbs": peak, "roofline_peak_source": peak_kind,
             "results": res, "clocks": clk, "verified": verified}
     if rank == 0:
@@ -802,6 +815,8 @@ def main():
     ap.add_argument("--workload", choices=["sssp_rmat22", "batch512", "grid4096", "rmat26", "er16"],
                     default="sssp_rmat22",
                     help="sssp_rmat22 is the benchmark line; the others are the other configurations")
+    ap.add_argument("--scale", type=int, default=26, help="rmat26 workload: RMAT scale")
+    ap.add_argument("--sources", type=int, default=64, help="rmat26 workload: BFS/SSSP sources")
     ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
                     help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
                          "host: one host launch per iteration; relaunch: one launch per iteration "
