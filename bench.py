@@ -733,7 +733,9 @@ def run_rmat26(args, rank: int, world: int, local: int):
     peak, peak_kind = peaks()
     clocks = Clocks(local)
     clocks.start()
-    for an, algo in (("bfs", i2.I2_BFS), ("sssp", i2.I2_SSSP), ("cc", i2.I2_CC)):
+    algos = [x for x in (("bfs", i2.I2_BFS), ("sssp", i2.I2_SSSP), ("cc", i2.I2_CC)) if x[0] in args.algos.split(",")]
+    keep = lambda name: args.rows == "all" or name in args.rows.split(",")
+    for an, algo in algos:
         # algorithmic bytes per traversal (reached counts of the first source:
         # every source with an edge lies in the giant component)
         rep = dg.run_device(algo, mine[0], variant="vp_cta", stream=sp)
@@ -743,7 +745,7 @@ def run_rmat26(args, rank: int, world: int, local: int):
         rows = [("vp_cta", "vp_cta", 0), ("heuristic", "heuristic", 0), ("learned", "learned", 0)]
         if algo == i2.I2_SSSP:
             rows.insert(1, ("vp_cta_budget", "vp_cta", i2.I2_SSSP_BUDGET_AUTO))
-        for name, v, budget in rows:
+        for name, v, budget in filter(lambda r: keep(r[0]), rows):
             ss = mine if algo != i2.I2_CC else mine[:1]
             run = lambda s_: dg.run_device(algo, s_, variant=v, loop=loop, stream=sp, report=False,
                                            budget=budget)
@@ -762,31 +764,37 @@ def run_rmat26(args, rank: int, world: int, local: int):
 
     host = dg.download()
     verified = {}
+    styles = [v for v in ("vp_cta", "heuristic", "learned") if keep(v)]
     for s_ in mine[:2]:
-        for v in ("vp_cta", "heuristic", "learned"):
+        for v in styles:
             for an, algo, wt in (("bfs", i2.I2_BFS, False), ("sssp", i2.I2_SSSP, True)):
+                if an not in args.algos.split(","):
+                    continue
                 d = dg._run(algo, s_, v, loop, 0, False, None)[0]
                 c = oracle.certify_distances(host, s_, d, weighted=wt)
                 if c is not None:
                     raise SystemExit(f"rmat26 {an} {v} source {s_}: certificate failed: {c}")
                 verified[f"{an}/{v}/src{s_}"] = "shortest-path certificate"
-        d = dg._run(i2.I2_SSSP, s_, "vp_cta", loop, 0, False, None, budget=i2.I2_SSSP_BUDGET_AUTO)[0]
-        c = oracle.certify_distances(host, s_, d, weighted=True)
-        if c is not None:
-            raise SystemExit(f"rmat26 sssp vp_cta_budget source {s_}: certificate failed: {c}")
-        verified[f"sssp/vp_cta_budget/src{s_}"] = "shortest-path certificate"
-    for v in ("vp_cta", "heuristic", "learned"):
+        if "sssp" in args.algos.split(",") and keep("vp_cta_budget"):
+            d = dg._run(i2.I2_SSSP, s_, "vp_cta", loop, 0, False, None, budget=i2.I2_SSSP_BUDGET_AUTO)[0]
+            c = oracle.certify_distances(host, s_, d, weighted=True)
+            if c is not None:
+                raise SystemExit(f"rmat26 sssp vp_cta_budget source {s_}: certificate failed: {c}")
+            verified[f"sssp/vp_cta_budget/src{s_}"] = "shortest-path certificate"
+    for v in styles if "cc" in args.algos.split(",") else ():
         lab = dg._run(i2.I2_CC, 0, v, loop, 0, False, None)[0]
         c = oracle.certify_cc(host, lab)
         if c is not None:
             raise SystemExit(f"rmat26 cc {v}: certificate failed: {c}")
         verified[f"cc/{v}"] = "minimum-label certificate"
     del host
-    line = {"metric": METRIC, "value": world * res["bfs/learned"]["gteps"], "unit": UNIT, "n_gpus": world,
+    head = res.get("bfs/learned") or next(iter(res.values()))
+    line = {"metric": METRIC, "value": world * head["gteps"], "unit": UNIT, "n_gpus": world,
             "steps": nsrc, "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",
-            "config": {"workload": f"rmat{args.scale}_bfs_sssp_cc_{nsrc}src", "nodes": dg.nodes,
-                       "edges": dg.edges, "generation_s": gen_s, "loop": args.loop,
+            "config": {"workload": f"rmat{args.scale}_{'_'.join(a for a, _ in algos)}_{nsrc}src",
+                       "nodes": dg.nodes, "edges": dg.edges, "generation_s": gen_s, "loop": args.loop,
+                       "rows": args.rows,
                        "parallelism": f"sources sharded x{world}"},
             "roofline_peak_gbs": peak, "roofline_peak_source": peak_kind,
             "results": res, "clocks": clk, "verified": verified}
@@ -817,6 +825,9 @@ def main():
                     help="sssp_rmat22 is the benchmark line; the others are the other configurations")
     ap.add_argument("--scale", type=int, default=26, help="rmat26 workload: RMAT scale")
     ap.add_argument("--sources", type=int, default=64, help="rmat26 workload: BFS/SSSP sources")
+    ap.add_argument("--algos", default="bfs,sssp,cc", help="rmat26 workload: algorithms to run")
+    ap.add_argument("--rows", default="all",
+                    help="rmat26 workload: rows to run (vp_cta, vp_cta_budget, heuristic, learned) or all")
     ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
                     help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
                          "host: one host launch per iteration; relaunch: one launch per iteration "

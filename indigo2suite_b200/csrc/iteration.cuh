@@ -50,7 +50,10 @@ static __device__ int heuristic_pick(const GStats& gs, int algo, int allowed, in
 // The learned selector is re-evaluated when the frontier's entries or edges
 // moved by more than a factor 1.5 since its last evaluation, or 16 iterations
 // passed; otherwise the previous choice stands (long tails of small, similar
-// frontiers do not pay for an inference each).
+// frontiers do not pay for an inference each). On graphs with more vertices
+// than any it was trained on it defers to the frequency rule (no inference):
+// measured on RMAT-24 and RMAT-26 BFS, its picks there cost 1.08-1.38x the
+// rule's time even with the size features clamped to the training range.
 static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool cond, int force) {
   __shared__ float x[kFeatures], h1[kHidden], h2[kHidden], y[kOut];
   __shared__ int s_eval;
@@ -69,7 +72,8 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
   }
   __syncthreads();
   const int mode = ctl->mode;
-  const bool infer = mode == 2 && c.mlp && cond && s_eval && force < 0;
+  const bool learned = c.mlp && c.gs.nodes <= kMaxTrainedNodes;
+  const bool infer = mode == 2 && learned && cond && s_eval && force < 0;
   if (infer) mlp_forward_block(c.mlp, x, h1, h2, y);
   if (threadIdx.x == 0) {
     int v = ctl->fixed_variant;
@@ -77,7 +81,7 @@ static __device__ void select_next(const Ctx& c, int next_iter, int nxt, bool co
       v = next_iter >= ctl->then_at ? ctl->then_variant : ctl->fixed_variant;
     } else if ((mode == 1 || mode == 2) && union_find_first(c.gs, ctl->algo, ctl->allowed, next_iter)) {
       v = kUnionFind;
-    } else if (mode == 1 || (mode == 2 && !c.mlp)) {
+    } else if (mode == 1 || (mode == 2 && !learned)) {
       volatile Slot* sl = &ctl->slot[nxt];
       const unsigned long long p = sl->packed;
       v = heuristic_pick(c.gs, ctl->algo, ctl->allowed, slot_size(p), slot_edges(p));

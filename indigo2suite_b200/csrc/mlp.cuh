@@ -24,9 +24,17 @@ constexpr int kOffB3 = kOffW3 + kHidden * kOut;
 constexpr int kParams = kOffB3 + kOut;
 
 // Features of a frontier about to be consumed. All are finite and O(1..30).
-// The graph-size features are clamped to 2^16..2^26 vertices and 2^17..2^31
-// CSR entries (the range from the training graphs to RMAT-26), and the
-// iteration index to 64 (frontiers reach their steady state by then).
+// The features that grow with the graph (frontier size and edges, largest
+// degrees, vertex and CSR-entry counts) are clamped to the largest values of
+// the training sweep (graphs of up to 2^21 vertices, 2^25.9 CSR entries,
+// degree 2^16.7): a larger graph is read as the largest one trained on
+// instead of extrapolating the network. The iteration index is clamped to 64
+// (frontiers reach their steady state by then).
+constexpr float kCapLogV = 21.f;     // log2 vertices
+constexpr long long kMaxTrainedNodes = 1LL << 21;  // the largest training graph's vertices
+constexpr float kCapLogE = 26.f;     // log2 CSR entries (frontier edges too)
+constexpr float kCapLogDeg = 17.f;   // log2 degree
+__device__ __forceinline__ float capf(float x, float hi) { return fminf(x, hi); }
 __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, int iter, int size, int hsize,
                                                   unsigned long long edges, int maxdeg, long long visited,
                                                   float* f) {
@@ -34,18 +42,18 @@ __device__ __forceinline__ void frontier_features(const GStats& gs, int algo, in
   const float fe = (float)edges;
   const float V = (float)gs.nodes;
   const float E = (float)gs.edges > 0.f ? (float)gs.edges : 1.f;
-  f[0] = log2f(1.f + fs);
-  f[1] = log2f(1.f + fe);
+  f[0] = capf(log2f(1.f + fs), kCapLogV);
+  f[1] = capf(log2f(1.f + fe), kCapLogE);
   f[2] = fs / V;
   f[3] = fe / E;
   f[4] = log2f(1.f + fe / fmaxf(1.f, fs));
-  f[5] = log2f(1.f + (float)maxdeg);
+  f[5] = capf(log2f(1.f + (float)maxdeg), kCapLogDeg);
   f[6] = (float)visited / V;
   f[7] = log2f(1.f + fminf((float)iter, 64.f));
-  f[8] = fminf(fmaxf(log2f(V), 16.f), 26.f);
-  f[9] = fminf(fmaxf(log2f(1.f + (float)gs.edges), 17.f), 31.f);
+  f[8] = fminf(fmaxf(log2f(V), 16.f), kCapLogV);
+  f[9] = fminf(fmaxf(log2f(1.f + (float)gs.edges), 17.f), kCapLogE);
   f[10] = log2f(1.f + gs.avgdeg);
-  f[11] = log2f(1.f + (float)gs.maxdeg);
+  f[11] = capf(log2f(1.f + (float)gs.maxdeg), kCapLogDeg);
   f[12] = log2f(1.f + gs.degcv);
   f[13] = algo == kSSSP ? 1.f : 0.f;
   f[14] = algo == kCC ? 1.f : 0.f;
