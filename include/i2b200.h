@@ -56,8 +56,15 @@ enum { I2_BFS = 0, I2_SSSP = 1, I2_CC = 2, I2_MIS = 3 };
 
 /* Relaxation variants (styles). Every variant reaches the same fixed point. */
 enum {
-  I2_AUTO_HEURISTIC = -1, /* per-iteration choice by a fixed frontier-size rule */
-  I2_AUTO_LEARNED = -2,   /* per-iteration choice by the on-device MLP selector */
+  I2_AUTO_HEURISTIC = -1, /* per-iteration choice by a fixed frontier-size rule; CC on
+                             symmetric graphs takes union-find, and single-source SSSP on
+                             graphs of skewed degrees with 2^26 CSR entries or more takes
+                             I2_VP_CTA in the budgeted near/far ordering (sssp_budget, the
+                             engine's default when 0), both chosen before the first launch */
+  I2_AUTO_LEARNED = -2,   /* per-iteration choice by the on-device MLP selector, with the
+                             same two choices made before the first launch; on graphs with
+                             more vertices than any it was trained on (2^21) it defers to
+                             the frequency rule */
   I2_VP_THREAD = 0,       /* vertex push, data-driven, thread per frontier vertex */
   I2_VP_WARP = 1,         /* vertex push, data-driven, warp per frontier vertex */
   I2_VP_CTA = 2,          /* edge-balanced push: thread per frontier edge */

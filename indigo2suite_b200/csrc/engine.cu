@@ -797,6 +797,10 @@ constexpr int kBudgetEdgesPerSM = 28672;
 // that wins moves with the graph. The edge budget instead keeps each near
 // frontier at about B edges: enough to fill the GPU, few enough that
 // distances settle before their vertices relax.
+// Smallest graph (CSR entries) on which the selectors' SSSP takes the budgeted
+// ordering (skewed degrees only; see run_traversal).
+constexpr long long kBudgetRuleEdges = 1LL << 26;
+
 static int pick_order(const i2_graph* g, int algo, int mode, int variant, int step, int budget) {
   if (algo != I2_SSSP || mode != 0 || variant != kVPCta) return 0;
   if (step > 0) return step;
@@ -1048,6 +1052,19 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   if (o.then_at > 0) {  // a fixed switch of style: per-iteration dispatch
     if (mode != 0 || o.then_variant < 0 || o.then_variant >= kNumVariants) return I2_ERR_ARG;
     mode = 3;
+  }
+  // SSSP on a graph of skewed degrees (coefficient of variation above 1) with
+  // 2^26 CSR entries or more, from one source: both selectors run the
+  // edge-balanced push in the budgeted near/far ordering for the whole
+  // traversal (the per-iteration styles cannot take part in its moves and
+  // trims). Measured against plain frontier-driven relaxation: 1.13x faster on
+  // RMAT-22 and 1.31x on RMAT-26; 5-28% slower on ER, grid and RMAT graphs of
+  // up to 2^21 vertices and 2^25 entries, which keep the per-iteration rule.
+  if (algo == I2_SSSP && (mode == 1 || mode == 2) && !srcs_host && o.sssp_delta <= 0 &&
+      (long long)g->g.edges >= kBudgetRuleEdges && g->gs.degcv > 1.f) {
+    mode = 0;
+    variant = kVPCta;
+    if (o.sssp_budget <= 0) o.sssp_budget = I2_SSSP_BUDGET_AUTO;
   }
   if (mode != 0 || variant == kEdgeTopo) {
     st = ensure_sp(g);

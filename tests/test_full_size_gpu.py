@@ -41,6 +41,31 @@ def test_rmat22_sssp_bit_exact(gpu, rmat22):
     assert oracle.certify_distances(g, src, d, weighted=True) is None
 
 
+def test_rmat22_selectors_take_the_budgeted_ordering(gpu, rmat22):
+    # A skewed graph of 2^26 CSR entries or more: both selectors run SSSP as
+    # the edge-balanced push in the budgeted near/far ordering (the records
+    # show its moves), with the oracle's distances. A skewed graph below that
+    # size keeps the per-iteration rule (relaxations only).
+    dg, g = rmat22
+    assert g.edges >= 1 << 26
+    src = int(np.argmax(g.degrees()))
+    ref = oracle.sssp(g, src)
+    for v in ("heuristic", "learned"):
+        d, rep = dg.sssp(src, variant=v, record=True)
+        np.testing.assert_array_equal(d, ref, err_msg=v)
+        kinds = {r["kind"] for r in dg.records()}
+        assert 1 in kinds, (v, kinds)
+        assert rep.variant_hist[i2.VARIANTS.index("vp_cta")] == rep.iterations
+    small = i2.gen_rmat(16, 16, seed=16)
+    ds = i2.DeviceGraph.upload(small)
+    s0 = int(np.argmax(small.degrees()))
+    for v in ("heuristic", "learned"):
+        d, _ = ds.sssp(s0, variant=v, record=True)
+        np.testing.assert_array_equal(d, oracle.sssp(small, s0), err_msg=v)
+        assert {r["kind"] for r in ds.records()} == {0}, v
+    ds.free()
+
+
 def test_rmat22_bfs_and_cc(gpu, rmat22):
     dg, g = rmat22
     src = int(np.argmax(g.degrees()))
