@@ -902,6 +902,14 @@ struct EpiStage {
 #ifndef I2_EB_MIN_BLOCKS
 #define I2_EB_MIN_BLOCKS 6
 #endif
+// Resident blocks per SM that the selectors' kernels (every style in one
+// kernel) are compiled for: 4 leaves them 64 registers, where 6 (the fixed
+// styles' 40) spilled 160-224 bytes per thread. Held-out RMAT/ER/grid graphs
+// of 2^18 and 2^20 vertices, geomean time against 6: BFS 0.90, SSSP 0.97-0.98,
+// CC 0.97-0.98 for both selectors (5 blocks: 0.93-0.98).
+#ifndef I2_SEL_MIN_BLOCKS
+#define I2_SEL_MIN_BLOCKS 4
+#endif
 
 struct EBShared {
   EpiStage s;
@@ -1692,7 +1700,7 @@ __device__ __forceinline__ bool run_body(const Ctx& c, AnyShared<DEFER>& sh) {
 // VAR >= 0: that style every iteration; VAR < 0: the style picked for each
 // iteration by the previous one (heuristic or learned selector).
 template <int ALG, int VAR, bool DEFER = false>
-__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_resident(Ctx c) {
+__global__ void __launch_bounds__(kBlock, VAR < 0 ? I2_SEL_MIN_BLOCKS : I2_EB_MIN_BLOCKS) relax_resident(Ctx c) {
   __shared__ AnyShared<DEFER> sh;
   __shared__ int s_go;
   Ctl* ctl = c.ctl;
@@ -1725,7 +1733,7 @@ __global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_resident(Ctx c
 }
 
 template <int ALG>
-__global__ void __launch_bounds__(kBlock, I2_EB_MIN_BLOCKS) relax_dispatch(Ctx c) {
+__global__ void __launch_bounds__(kBlock, I2_SEL_MIN_BLOCKS) relax_dispatch(Ctx c) {
   __shared__ AnyShared<> sh;
   switch (c.ctl->variant) {  // same value for every thread of the launch
     case kVPThread: body_push<ALG, kVPThread>(c, sh.st); break;
