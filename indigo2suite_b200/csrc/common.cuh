@@ -182,6 +182,19 @@ struct Ctl {
   float feat[kFeatures];    // features of the frontier the next launch consumes
 };
 
+// Union-find CC pays on graphs of 2^19 vertices or more, or of average degree
+// below 6 (measured 2.5-23x faster than the best propagation style on RMAT,
+// ER and grid graphs of 2^22 vertices and more; propagation up to 1.7x faster
+// on RMAT and ER of 2^18 vertices with higher degrees). Both selectors take it
+// before the first iteration on symmetric graphs.
+__host__ __device__ inline bool union_find_pays(long long nodes, float avgdeg) {
+  return nodes >= (1LL << 19) || avgdeg < 6.f;
+}
+
+// Graphs on which the selectors' kernel is compiled for the fixed styles'
+// resident blocks per SM rather than I2_SEL_MIN_BLOCKS (relax.cuh).
+constexpr long long kWideSelectorNodes = 1LL << 25;
+
 enum : int {
   kStatusIterCap = 1,
   kStatusOverflow = 2,

@@ -322,10 +322,12 @@ static KernelFn relax_fn(int v) {
   return nullptr;
 }
 
-static KernelFn dispatch_kernel(int algo) {
-  if (algo == kBFS) return relax_dispatch<kBFS>;
-  if (algo == kSSSP) return relax_dispatch<kSSSP>;
-  return relax_dispatch<kCC>;  // MIS has one style and never dispatches
+// The selectors' per-iteration kernel; `wide`: the form compiled for the fixed
+// styles' resident blocks per SM (graphs of kWideSelectorNodes vertices or more).
+static KernelFn dispatch_kernel(int algo, bool wide) {
+  if (algo == kBFS) return wide ? relax_dispatch<kBFS, I2_EB_MIN_BLOCKS> : relax_dispatch<kBFS>;
+  if (algo == kSSSP) return wide ? relax_dispatch<kSSSP, I2_EB_MIN_BLOCKS> : relax_dispatch<kSSSP>;
+  return wide ? relax_dispatch<kCC, I2_EB_MIN_BLOCKS> : relax_dispatch<kCC>;  // MIS never dispatches
 }
 
 KernelFn relax_kernel(int algo, int v, bool near_far) {
@@ -746,6 +748,9 @@ static int ensure_symmetry(i2_graph* g) {
 // Styles applicable to this graph and algorithm: pull and union-find read a
 // vertex's out-list as its in-list (symmetric graphs only), the edge sweeps
 // need sp[], and union-find computes CC labels only.
+// Whether the selectors run in the form compiled for more resident blocks.
+static bool wide_selector(const i2_graph* g) { return (long long)g->g.nodes >= kWideSelectorNodes; }
+
 static int allowed_mask(const i2_graph* g, int algo) {
   int m = 0;
   for (int v = 0; v < kNumVariants; ++v) m |= 1 << v;
@@ -915,9 +920,9 @@ static int build_exec(i2_graph* g, int algo, int mode, int variant, bool multi, 
   // branch on the style the previous iteration selected.
   {
     cudaGraphNode_t n;
-    KernelFn fn = resident ? resident_kernel(algo, mode == 0 ? variant : -1, rp.delta != 0)
+    KernelFn fn = resident ? resident_kernel(algo, mode == 0 ? variant : -1, rp.delta != 0, wide_selector(g))
                   : mode == 0 ? relax_kernel(algo, variant, rp.delta != 0)
-                              : dispatch_kernel(algo);
+                              : dispatch_kernel(algo, wide_selector(g));
     st = add_kernel_node(body, &n, nullptr, 0, fn, grid_for(fn, g->blocks_per_sm), &c);
     if (st) return st;
     if (resident) {
@@ -1060,6 +1065,17 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   // trims). Measured against plain frontier-driven relaxation: 1.13x faster on
   // RMAT-22 and 1.31x on RMAT-26; 5-28% slower on ER, grid and RMAT graphs of
   // up to 2^21 vertices and 2^25 entries, which keep the per-iteration rule.
+  // CC on a symmetric graph where union-find pays: both selectors take it
+  // before the first iteration, so it runs as union-find's own kernel (the
+  // selectors' kernel, compiled for every style, measured up to 1.3x slower).
+  if (algo == I2_CC && (mode == 1 || mode == 2)) {
+    st = ensure_symmetry(g);
+    if (st) return st;
+    if (((allowed_mask(g, algo) >> kUnionFind) & 1) && union_find_pays(g->g.nodes, g->gs.avgdeg)) {
+      mode = 0;
+      variant = kUnionFind;
+    }
+  }
   if (algo == I2_SSSP && (mode == 1 || mode == 2) && !srcs_host && o.sssp_delta <= 0 &&
       (long long)g->g.edges >= kBudgetRuleEdges && g->gs.degcv > 1.f) {
     mode = 0;
@@ -1189,7 +1205,7 @@ static int sweep(i2_graph* g, int algo, int src, int follow, int reps, i2_iter_r
   Ctl snap;
   int it = 0;
   // Styles are timed through the dispatch kernel, the one the selectors run.
-  KernelFn dk = dispatch_kernel(algo);
+  KernelFn dk = dispatch_kernel(algo, wide_selector(g));
   const int dgrid = grid_for(dk, g->blocks_per_sm);
   while (it < cap) {
     I2_CK(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));

@@ -12,8 +12,9 @@ int cuda_status(cudaError_t e);
 int grid_for(KernelFn fn, int max_per_sm);
 KernelFn relax_kernel(int algo, int variant, bool near_far = false);
 // Resident traversal kernel: fixed style `variant`, or the per-iteration pick
-// when variant < 0 (resident.cu).
-KernelFn resident_kernel(int algo, int variant, bool near_far);
+// when variant < 0, in the form compiled for more resident blocks when `wide`
+// (resident.cu).
+KernelFn resident_kernel(int algo, int variant, bool near_far, bool wide = false);
 const float* mlp_device_params();
 int mlp_install(const float* params, int count);
 

@@ -24,8 +24,7 @@ namespace i2 {
 // faster than union-find; on grids and on every graph of 2^20 vertices and
 // more, union-find was the fastest.
 static __device__ bool union_find_first(const GStats& gs, int algo, int allowed, int next_iter) {
-  const bool big_or_sparse = gs.nodes >= (1 << 19) || gs.avgdeg < 6.f;
-  return algo == kCC && next_iter == 0 && ((allowed >> kUnionFind) & 1) && big_or_sparse;
+  return algo == kCC && next_iter == 0 && ((allowed >> kUnionFind) & 1) && union_find_pays(gs.nodes, gs.avgdeg);
 }
 
 // The learned selector overrides the rule only where it predicts the rule's

@@ -906,7 +906,11 @@ struct EpiStage {
 // kernel) are compiled for: 4 leaves them 64 registers, where 6 (the fixed
 // styles' 40) spilled 160-224 bytes per thread. Held-out RMAT/ER/grid graphs
 // of 2^18 and 2^20 vertices, geomean time against 6: BFS 0.90, SSSP 0.97-0.98,
-// CC 0.97-0.98 for both selectors (5 blocks: 0.93-0.98).
+// CC 0.97-0.98 for both selectors (5 blocks: 0.93-0.98); grid 4096² BFS 0.92.
+// On RMAT-26 the heuristic BFS took 1.21x as long at 4 blocks (its pull
+// iterations over 2^26 vertices need the warps), so graphs of
+// kWideSelectorNodes vertices or more get the selector kernel compiled for the
+// fixed styles' I2_EB_MIN_BLOCKS.
 #ifndef I2_SEL_MIN_BLOCKS
 #define I2_SEL_MIN_BLOCKS 4
 #endif
@@ -1699,8 +1703,8 @@ __device__ __forceinline__ bool run_body(const Ctx& c, AnyShared<DEFER>& sh) {
 
 // VAR >= 0: that style every iteration; VAR < 0: the style picked for each
 // iteration by the previous one (heuristic or learned selector).
-template <int ALG, int VAR, bool DEFER = false>
-__global__ void __launch_bounds__(kBlock, VAR < 0 ? I2_SEL_MIN_BLOCKS : I2_EB_MIN_BLOCKS) relax_resident(Ctx c) {
+template <int ALG, int VAR, bool DEFER = false, int MINB = (VAR < 0 ? I2_SEL_MIN_BLOCKS : I2_EB_MIN_BLOCKS)>
+__global__ void __launch_bounds__(kBlock, MINB) relax_resident(Ctx c) {
   __shared__ AnyShared<DEFER> sh;
   __shared__ int s_go;
   Ctl* ctl = c.ctl;
@@ -1732,8 +1736,8 @@ __global__ void __launch_bounds__(kBlock, VAR < 0 ? I2_SEL_MIN_BLOCKS : I2_EB_MI
   }
 }
 
-template <int ALG>
-__global__ void __launch_bounds__(kBlock, I2_SEL_MIN_BLOCKS) relax_dispatch(Ctx c) {
+template <int ALG, int MINB = I2_SEL_MIN_BLOCKS>
+__global__ void __launch_bounds__(kBlock, MINB) relax_dispatch(Ctx c) {
   __shared__ AnyShared<> sh;
   switch (c.ctl->variant) {  // same value for every thread of the launch
     case kVPThread: body_push<ALG, kVPThread>(c, sh.st); break;

@@ -10,7 +10,7 @@
 namespace i2 {
 
 template <int ALG>
-static KernelFn resident_fn(int v) {
+static KernelFn resident_fn(int v, bool wide) {
   switch (v) {
     case kVPThread: return relax_resident<ALG, kVPThread>;
     case kVPWarp: return relax_resident<ALG, kVPWarp>;
@@ -24,17 +24,18 @@ static KernelFn resident_fn(int v) {
       if constexpr (ALG == kCC) return relax_resident<ALG, kUnionFind>;
       return nullptr;
   }
-  return relax_resident<ALG, -1>;  // per-iteration pick
+  // per-iteration pick
+  return wide ? relax_resident<ALG, -1, false, I2_EB_MIN_BLOCKS> : relax_resident<ALG, -1>;
 }
 
 // Kernel of a resident traversal: fixed style v (mode 0) or the per-iteration
-// pick (v < 0).
-KernelFn resident_kernel(int algo, int v, bool near_far) {
+// pick (v < 0; `wide`: the form compiled for more resident blocks).
+KernelFn resident_kernel(int algo, int v, bool near_far, bool wide) {
   if (algo == kMIS) return relax_resident<kMIS, kVPWarp>;  // one style
   if (near_far && algo == kSSSP && v == kVPCta) return relax_resident<kSSSP, kVPCta, true>;
-  if (algo == kBFS) return resident_fn<kBFS>(v);
-  if (algo == kSSSP) return resident_fn<kSSSP>(v);
-  return resident_fn<kCC>(v);
+  if (algo == kBFS) return resident_fn<kBFS>(v, wide);
+  if (algo == kSSSP) return resident_fn<kSSSP>(v, wide);
+  return resident_fn<kCC>(v, wide);
 }
 
 }  // namespace i2
