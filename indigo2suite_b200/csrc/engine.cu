@@ -748,6 +748,10 @@ static int ensure_symmetry(i2_graph* g) {
 // Styles applicable to this graph and algorithm: pull and union-find read a
 // vertex's out-list as its in-list (symmetric graphs only), the edge sweeps
 // need sp[], and union-find computes CC labels only.
+// Smallest graph (vertices) on which the selectors' union-find CC runs as
+// union-find's own kernel (run_traversal).
+constexpr long long kUnionFindKernelNodes = 1LL << 22;
+
 // Whether the selectors run in the form compiled for more resident blocks.
 static bool wide_selector(const i2_graph* g) { return (long long)g->g.nodes >= kWideSelectorNodes; }
 
@@ -1065,10 +1069,13 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   // trims). Measured against plain frontier-driven relaxation: 1.13x faster on
   // RMAT-22 and 1.31x on RMAT-26; 5-28% slower on ER, grid and RMAT graphs of
   // up to 2^21 vertices and 2^25 entries, which keep the per-iteration rule.
-  // CC on a symmetric graph where union-find pays: both selectors take it
-  // before the first iteration, so it runs as union-find's own kernel (the
-  // selectors' kernel, compiled for every style, measured up to 1.3x slower).
-  if (algo == I2_CC && (mode == 1 || mode == 2)) {
+  // CC on a symmetric graph of 2^22 vertices or more where union-find pays:
+  // both selectors take it before the first iteration, so it runs as
+  // union-find's own kernel (grid 4096²: 1.37-1.47 ms against 1.79-1.89 in the
+  // selectors' kernel at 4 blocks per SM). On smaller graphs the selectors'
+  // kernel, with its 64 registers, measured faster (ER 2^20: 0.25 against
+  // 0.33 ms; grid 2^18: 0.14 against 0.22-0.28).
+  if (algo == I2_CC && (mode == 1 || mode == 2) && (long long)g->g.nodes >= kUnionFindKernelNodes) {
     st = ensure_symmetry(g);
     if (st) return st;
     if (((allowed_mask(g, algo) >> kUnionFind) & 1) && union_find_pays(g->g.nodes, g->gs.avgdeg)) {
