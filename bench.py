@@ -703,7 +703,8 @@ def run_rmat26(args, rank: int, world: int, local: int):
     """Config: RMAT scale 26 (--scale), 64 seeded sources (--sources; degree
     >= 1) for BFS and SSSP, CC once; the edge-balanced fixed style (SSSP also
     with the budgeted near/far ordering), the heuristic and the learned
-    selector. Sources shard across ranks."""
+    selector; BFS and SSSP on the graph's degree-ordered copy unless --order
+    none. Sources shard across ranks."""
     import torch
 
     import indigo2suite_b200 as i2
@@ -719,6 +720,11 @@ def run_rmat26(args, rank: int, world: int, local: int):
     nsrc = args.sources
     dg = i2.DeviceGraph.generate_rmat(args.scale, 16, 0.57, 0.19, 0.19, seed=args.scale)
     gen_s = time.time() - t0
+    # BFS and SSSP on the degree-ordered copy (CC keeps the original CSR)
+    t1 = time.time()
+    dg.reorder(args.order)
+    torch.cuda.synchronize()
+    order_s = time.time() - t1
     if SELECTOR_PARAMS.exists():
         i2.mlp_set_params(np.fromfile(SELECTOR_PARAMS, np.float32))
     rng = np.random.default_rng(args.scale)
@@ -794,6 +800,7 @@ def run_rmat26(args, rank: int, world: int, local: int):
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": f"rmat{args.scale}_{'_'.join(a for a, _ in algos)}_{nsrc}src",
                        "nodes": dg.nodes, "edges": dg.edges, "generation_s": gen_s, "loop": args.loop,
+                       "vertex_order": args.order, "reorder_s": order_s,
                        "rows": args.rows,
                        "parallelism": f"sources sharded x{world}"},
             "roofline_peak_gbs": peak, "roofline_peak_source": peak_kind,
@@ -828,6 +835,9 @@ def main():
     ap.add_argument("--algos", default="bfs,sssp,cc", help="rmat26 workload: algorithms to run")
     ap.add_argument("--rows", default="all",
                     help="rmat26 workload: rows to run (vp_cta, vp_cta_budget, heuristic, learned) or all")
+    ap.add_argument("--order", choices=["none", "degree"], default="degree",
+                    help="rmat26 workload: vertex numbering BFS and SSSP run under (degree: a copy "
+                         "renumbered by descending degree, results in original IDs)")
     ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
                     help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
                          "host: one host launch per iteration; relaunch: one launch per iteration "

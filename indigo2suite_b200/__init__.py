@@ -306,6 +306,13 @@ class DeviceGraph:
     def tune(self, heavy_threshold: int = 0, blocks_per_sm: int = 0, smem_carveout: int = -1) -> None:
         _check(lib.i2_graph_tune(self._h, heavy_threshold, blocks_per_sm, smem_carveout), "tune")
 
+    def reorder(self, order: str = "degree") -> None:
+        """Run BFS and SSSP on a copy of the graph renumbered by descending
+        degree ("degree"), or drop that copy ("none"). Results stay in the
+        original IDs and equal the original CSR's."""
+        code = {"none": capi.I2_ORDER_NONE, "degree": capi.I2_ORDER_DEGREE}[order]
+        _check(lib.i2_graph_reorder(self._h, code), "reorder")
+
     def synth_weights(self) -> None:
         _check(lib.i2_graph_synth_weights(self._h), "synth weights")
 

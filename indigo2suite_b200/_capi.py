@@ -32,6 +32,8 @@ MIS_IN, MIS_OUT = 1, 2  # status values of i2_mis (the reference's included / ex
 I2_AUTO_HEURISTIC = -1
 I2_AUTO_LEARNED = -2
 I2_SSSP_BUDGET_AUTO = -1
+I2_ORDER_NONE = 0
+I2_ORDER_DEGREE = 1
 VARIANTS = ["vp_thread", "vp_warp", "vp_cta", "vp_block", "pull_frontier", "pull_topo", "edge_topo", "push_topo",
             "union_find"]
 I2_NUM_VARIANTS = len(VARIANTS)
@@ -110,6 +112,7 @@ SIGNATURES = {
     "i2_graph_download": (_I, [_P, _PG]),
     "i2_graph_synth_weights": (_I, [_P]),
     "i2_graph_tune": (_I, [_P, _I, _I, _I]),
+    "i2_graph_reorder": (_I, [_P, _I]),
     "i2_gen_rmat_n": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64, _I, _PG]),
     "i2_graph_free": (_I, [_P]),
     "i2_trim_device_memory": (_I, []),

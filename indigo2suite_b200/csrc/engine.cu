@@ -299,6 +299,14 @@ __global__ void k_reached(DGraph g, const int* dist, unsigned long long* out) {
   }
 }
 
+// Values of a traversal on the degree-ordered copy, back in original IDs:
+// out[v] = copy[inv[v]] (coalesced inv read and write, gathered copy read).
+__global__ void k_unpermute(const int* __restrict__ copy, const int* __restrict__ inv, int n,
+                            int* __restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) out[v] = copy[inv[v]];
+}
+
 // ---------------------------------------------------------------------------
 // Kernel tables.
 
@@ -484,6 +492,12 @@ struct i2_graph {
   unsigned* snap_bm = nullptr;
   int* snap_wl = nullptr;
   int* snap_hwl = nullptr;
+  // degree-ordered copy (i2_graph_reorder): BFS and SSSP run on it, their
+  // sources mapped by inv and their results gathered back to original IDs
+  i2_graph* twin = nullptr;
+  int* d_inv = nullptr;         // original ID -> copy's ID (device)
+  std::vector<int> h_inv;       // the same on the host, to map sources
+  bool last_on_twin = false;    // the last traversal ran on the copy (records)
 };
 
 namespace i2 {
@@ -620,6 +634,10 @@ static void free_graph_state(i2_graph* g) {
   if (g->ev3) cudaEventDestroy(g->ev3);
   if (g->stream) cudaStreamDestroy(g->stream);
   dev_free(g->d_sp);
+  if (g->twin) i2_graph_free(g->twin);
+  g->twin = nullptr;
+  dev_free(g->d_inv);
+  g->d_inv = nullptr;
   if (g->owns) {
     dev_free(g->d_nindex);
     dev_free(g->d_nlist);
@@ -1028,11 +1046,58 @@ static int fill_report(i2_graph* g, cudaStream_t s, int algo, i2_report* rep, do
   return I2_OK;
 }
 
+// BFS or SSSP of a graph that has a degree-ordered copy: the traversal runs
+// on the copy (same options, on the caller's stream or the graph's), from the
+// mapped sources, and one gather puts its values into this graph's result
+// buffer in original IDs. Levels and distances do not depend on the
+// numbering, so the result is the one the original CSR gives. The report's
+// seconds cover the traversal and the gather.
+static int run_on_twin(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
+                       i2_report* rep) {
+  std::vector<int> mapped;
+  if (srcs_host) {
+    if (nsrc < 1) return I2_ERR_ARG;
+    mapped.resize(nsrc);
+    for (int j = 0; j < nsrc; ++j) {
+      if (srcs_host[j] < 0 || srcs_host[j] >= g->g.nodes) return I2_ERR_ARG;
+      mapped[j] = g->h_inv[srcs_host[j]];
+    }
+  } else if (src < 0 || src >= g->g.nodes) {
+    return I2_ERR_ARG;
+  }
+  int st = ensure_workspace(g);
+  if (st) return st;
+  i2_opts o{};
+  if (opts) o = *opts;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
+  o.stream = (void*)s;
+  if (rep) I2_CK(cudaEventRecord(g->ev2, s));
+  st = run_traversal(g->twin, algo, srcs_host ? 0 : g->h_inv[src], srcs_host ? mapped.data() : nullptr, nsrc, &o,
+                     rep);
+  if (st && st != I2_ERR_ITER_CAP) return st;
+  g->last_on_twin = true;
+  g->last_iters = g->twin->last_iters;
+  const int n = g->g.nodes;
+  k_unpermute<<<(int)std::min<long long>(4LL * sm_count(), (n + 255) / 256), 256, 0, s>>>(g->twin->dist, g->d_inv, n,
+                                                                                          g->dist);
+  I2_CK(cudaGetLastError());
+  if (rep) {
+    I2_CK(cudaEventRecord(g->ev3, s));
+    I2_CK(cudaEventSynchronize(g->ev3));
+    float ms = 0.f;
+    I2_CK(cudaEventElapsedTime(&ms, g->ev2, g->ev3));
+    rep->seconds = ms * 1e-3;
+  }
+  return st;
+}
+
 int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
                   i2_report* rep) {
   if (!g) return I2_ERR_ARG;
   if (algo < I2_BFS || algo > I2_MIS) return I2_ERR_ARG;
   I2_CK(cudaSetDevice(g->device));
+  if (g->twin && (algo == I2_BFS || algo == I2_SSSP)) return run_on_twin(g, algo, src, srcs_host, nsrc, opts, rep);
+  g->last_on_twin = false;
   i2_opts o{};
   if (opts) o = *opts;
   if (o.loop_mode < I2_LOOP_GRAPH || o.loop_mode > I2_LOOP_RELAUNCH) return I2_ERR_ARG;
@@ -1585,6 +1650,7 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_
         I2_CK(dev_alloc(&g->htoff[k], sizeof(unsigned) * std::max(1, g->gs.nheavy)));
       }
   }
+  if (g->twin) return i2_graph_tune(g->twin, heavy_threshold, blocks_per_sm, smem_carveout);
   return I2_OK;
 }
 
@@ -1601,7 +1667,10 @@ int i2_graph_synth_weights(i2_graph* g) {
   g->g.eweight = w;
   g->g.vec_ok = ((((uintptr_t)g->g.nlist) & 15) == 0 && (((uintptr_t)w) & 15) == 0) ? 1 : 0;
   drop_execs(g);
-  return compute_stats(g);
+  const int st = compute_stats(g);
+  if (st || !g->twin) return st;
+  // the weights are a function of the original IDs: renumber again
+  return i2_graph_reorder(g, I2_ORDER_DEGREE);
 }
 
 int i2_graph_free(i2_graph* g) {
@@ -1610,6 +1679,45 @@ int i2_graph_free(i2_graph* g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   free_graph_state(g);
   delete g;
+  return I2_OK;
+}
+
+int i2_graph_reorder(i2_graph* g, int order) {
+  if (!g || (order != I2_ORDER_NONE && order != I2_ORDER_DEGREE)) return I2_ERR_ARG;
+  I2_CK(cudaSetDevice(g->device));
+  if (g->stream) I2_CK(cudaStreamSynchronize(g->stream));
+  if (g->twin) {
+    i2_graph_free(g->twin);
+    g->twin = nullptr;
+    dev_free(g->d_inv);
+    g->d_inv = nullptr;
+    g->h_inv.clear();
+    g->h_inv.shrink_to_fit();
+    g->last_on_twin = false;
+  }
+  if (order == I2_ORDER_NONE) return I2_OK;
+  i2_graph* twin = nullptr;
+  int* inv = nullptr;
+  int st = degree_ordered_copy(g, &twin, &inv);
+  if (st) return st;
+  std::vector<int> h(g->g.nodes);
+  const cudaError_t e = cudaMemcpy(h.data(), inv, sizeof(int) * h.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    i2_graph_free(twin);
+    dev_free(inv);
+    return cuda_status(e);
+  }
+  // the copy launches like the original (settings of i2_graph_tune; the
+  // heavy lists are sized for the threshold by the tune call)
+  st = i2_graph_tune(twin, g->heavy, g->blocks_per_sm, g_carveout);
+  if (st) {
+    i2_graph_free(twin);
+    dev_free(inv);
+    return st;
+  }
+  g->twin = twin;
+  g->d_inv = inv;
+  g->h_inv.swap(h);
   return I2_OK;
 }
 
@@ -1654,6 +1762,7 @@ int i2_run_device(i2_graph* g, int algo, int src, int* out_dev, const i2_opts* o
 
 int i2_get_records(const i2_graph* g, i2_iter_record* out, int cap, int* n) {
   if (!g || !out || !n || cap < 0) return I2_ERR_ARG;
+  if (g->last_on_twin && g->twin) return i2_get_records(g->twin, out, cap, n);
   if (!g->ws_ready) {
     *n = 0;
     return I2_OK;

@@ -35,6 +35,11 @@ int graph_adopt(int nodes, int edges, int* d_nindex, int* d_nlist, int* d_eweigh
 int graph_device_csr(const i2_graph* g, int* nodes, int* edges, const int** nindex, const int** nlist,
                      const int** eweight);
 
+// A copy of g with its vertices renumbered by descending degree, ties by
+// ascending ID (gen_device.cu): *twin is a new graph, *inv (g.nodes ints,
+// from dev_alloc) maps each original ID to the copy's.
+int degree_ordered_copy(const i2_graph* g, i2_graph** twin, int** inv);
+
 // Copy the last traversal's values to a host array of g.nodes ints.
 int graph_copy_result(i2_graph* g, int* host_out, const i2_opts* opts);
 

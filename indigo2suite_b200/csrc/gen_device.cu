@@ -79,10 +79,13 @@ struct MinOp {
 // Scratch of a build, freed on every path (plain allocations: transient, so
 // the engine's pool never keeps them).
 struct Scratch {
-  void* p[8] = {nullptr};
+  static constexpr int kMax = 16;
+  void* p[kMax] = {nullptr};
   int n = 0;
   template <class T>
   cudaError_t get(T** out, size_t bytes) {
+    *out = nullptr;
+    if (n == kMax) return cudaErrorMemoryAllocation;  // more buffers than one build takes
     void* q = nullptr;
     const cudaError_t e = cudaMalloc(&q, bytes > 0 ? bytes : 1);
     if (e == cudaSuccess) p[n++] = q;
@@ -457,3 +460,99 @@ extern "C" int i2_graph_from_coo_device(int nodes, long long m, const int* src, 
   if (hbad) return I2_ERR_FORMAT;
   return csr_from_keys(k0, k1, w0, w1, nkeys, nodes, CutWeights{w ? 2 : 0, 0, nullptr}, out);
 }
+
+// ---------------------------------------------------------------------------
+// Degree-ordered copy of a graph: vertex IDs renumbered by descending degree
+// (ties by ascending ID), so that the few vertices most adjacency lists name
+// sit together at the front of every per-vertex array. On RMAT the generator
+// scatters its hubs over the whole ID range, and once dist[] outgrows L2 (2^25
+// vertices and more) the neighbours' random dist reads and atomicMins miss;
+// renumbered, the vertices that take most of those accesses fit in L2.
+
+namespace i2 {
+namespace {
+
+__global__ void k_degree_ids(const int* __restrict__ nindex, int n, int* __restrict__ deg, int* __restrict__ ids) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    deg[v] = nindex[v + 1] - nindex[v];
+    ids[v] = v;
+  }
+}
+
+__global__ void k_invert(const int* __restrict__ perm, int n, int* __restrict__ inv) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv[perm[i]] = i;
+}
+
+// One warp per vertex (grid-stride): every CSR entry e of old vertex u becomes
+// the key (inv[u] << 32 | inv[nlist[e]]) at position e, its weight beside it.
+__global__ void k_relabel_keys(const int* __restrict__ nindex, const int* __restrict__ nlist,
+                               const int* __restrict__ w, const int* __restrict__ inv, int n,
+                               unsigned long long* __restrict__ keys, int* __restrict__ wk) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long u = warp; u < n; u += nwarps) {
+    const unsigned long long hi = (unsigned long long)(unsigned)inv[u] << 32;
+    const int beg = nindex[u], end = nindex[u + 1];
+    for (int e = beg + lane; e < end; e += 32) {
+      const int v = nlist[e];  // in range in every graph handle; dropped if not
+      keys[e] = (unsigned)v < (unsigned)n ? (hi | (unsigned)inv[v]) : kDropKey;
+      if (w) wk[e] = w[e];
+    }
+  }
+}
+
+}  // namespace
+
+int degree_ordered_copy(const i2_graph* g, i2_graph** twin, int** inv_out) {
+  *twin = nullptr;
+  *inv_out = nullptr;
+  int n = 0, E = 0;
+  const int *nindex = nullptr, *nlist = nullptr, *w = nullptr;
+  int st = graph_device_csr(g, &n, &E, &nindex, &nlist, &w);
+  if (st) return st;
+  Scratch sc;
+  int *deg = nullptr, *ids = nullptr, *deg_sorted = nullptr, *perm = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  cudaError_t e = sc.get(&deg, sizeof(int) * (size_t)n);
+  if (e == cudaSuccess) e = sc.get(&ids, sizeof(int) * (size_t)n);
+  if (e == cudaSuccess) e = sc.get(&deg_sorted, sizeof(int) * (size_t)n);
+  if (e == cudaSuccess) e = sc.get(&perm, sizeof(int) * (size_t)n);
+  if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg, deg_sorted, ids, perm, n);
+  if (e == cudaSuccess) e = sc.get(&tmp, tb);
+  if (e != cudaSuccess) return cuda_status(e);
+  k_degree_ids<<<1024, 256>>>(nindex, n, deg, ids);
+  // LSD radix sort is stable: equal degrees keep ascending IDs
+  e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, deg, deg_sorted, ids, perm, n);
+  int* inv = nullptr;
+  if (e == cudaSuccess) e = dev_alloc(&inv, sizeof(int) * (size_t)n);
+  if (e != cudaSuccess) return cuda_status(e);
+  k_invert<<<1024, 256>>>(perm, n, inv);
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  int *w0 = nullptr, *w1 = nullptr;
+  const size_t nk = (size_t)(E > 0 ? E : 1);
+  e = sc.get(&k0, sizeof(unsigned long long) * nk);
+  if (e == cudaSuccess) e = sc.get(&k1, sizeof(unsigned long long) * nk);
+  if (e == cudaSuccess && w) e = sc.get(&w0, sizeof(int) * nk);
+  if (e == cudaSuccess && w) e = sc.get(&w1, sizeof(int) * nk);
+  if (e == cudaSuccess) {
+    k_relabel_keys<<<4096, 256>>>(nindex, nlist, w, inv, n, k0, w0);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    dev_free(inv);
+    return cuda_status(e);
+  }
+  st = csr_from_keys(k0, k1, w0, w1, E, n, CutWeights{w ? 2 : 0, 0, nullptr}, twin);
+  if (st) {
+    dev_free(inv);
+    return st;
+  }
+  *inv_out = inv;
+  return I2_OK;
+}
+
+}  // namespace i2

@@ -51,16 +51,26 @@ def test_rmat26_certificates(gpu):
     try:
         assert dg.nodes == 1 << 26 and 2_000_000_000 < dg.edges <= 2**31 - 1
         g = dg.download()
+        certified = {}
         for src in rmat26_sources(dg, 2):
             for v in ("vp_cta", "heuristic", "learned"):
                 d = dg.bfs(src, variant=v)[0]
                 assert oracle.certify_distances(g, src, d, weighted=False) is None, f"bfs {v} {src}"
+            certified["bfs", src] = d
             # the selectors take the budgeted near/far ordering at this size
             for v in ("vp_cta", "heuristic"):
                 d = dg.sssp(src, variant=v)[0]
                 assert oracle.certify_distances(g, src, d, weighted=True) is None, f"sssp {v} {src}"
+            certified["sssp", src] = d
         for v in ("union_find", "heuristic"):
             lab = dg.cc(variant=v)[0]
             assert oracle.certify_cc(g, lab) is None, f"cc {v}"
+        # the degree-ordered copy gives the certified values, in original IDs
+        dg.reorder("degree")
+        for (algo, src), want in certified.items():
+            for v in ("vp_cta", "heuristic"):
+                got = (dg.bfs if algo == "bfs" else dg.sssp)(src, variant=v)[0]
+                np.testing.assert_array_equal(got, want, err_msg=f"reordered {algo} {v} {src}")
+        np.testing.assert_array_equal(dg.cc(variant="heuristic")[0], lab, err_msg="cc after reorder")
     finally:
         dg.free()
