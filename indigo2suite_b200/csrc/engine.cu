@@ -307,6 +307,33 @@ __global__ void k_unpermute(const int* __restrict__ copy, const int* __restrict_
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) out[v] = copy[inv[v]];
 }
 
+// CC on the degree-ordered copy labels each vertex with its component's
+// smallest copy ID; the caller's labels are the smallest original IDs. First
+// mn[r] = min { v : label of copy vertex inv[v] is r } (one atomicMin per
+// distinct label in a warp, by its lowest lane, which holds the smallest v
+// since a warp covers consecutive v; skipped when mn[r] is already smaller,
+// as it soon is for the giant component), then out[v] = mn[label(inv[v])].
+__global__ void k_cc_min_init(int* __restrict__ mn, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) mn[v] = INT_MAX;
+}
+
+__global__ void k_cc_min_original(const int* __restrict__ copy_label, const int* __restrict__ inv, int n,
+                                  int* mn) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const int r = copy_label[inv[v]];
+    const unsigned peers = __match_any_sync(__activemask(), r);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && v < *(volatile int*)&mn[r]) atomicMin(&mn[r], v);
+  }
+}
+
+__global__ void k_cc_labels(const int* __restrict__ copy_label, const int* __restrict__ inv,
+                            const int* __restrict__ mn, int n, int* __restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) out[v] = mn[copy_label[inv[v]]];
+}
+
 // ---------------------------------------------------------------------------
 // Kernel tables.
 
@@ -1046,12 +1073,13 @@ static int fill_report(i2_graph* g, cudaStream_t s, int algo, i2_report* rep, do
   return I2_OK;
 }
 
-// BFS or SSSP of a graph that has a degree-ordered copy: the traversal runs
-// on the copy (same options, on the caller's stream or the graph's), from the
-// mapped sources, and one gather puts its values into this graph's result
-// buffer in original IDs. Levels and distances do not depend on the
-// numbering, so the result is the one the original CSR gives. The report's
-// seconds cover the traversal and the gather.
+// BFS, SSSP or (symmetric graphs) CC of a graph that has a degree-ordered
+// copy: the traversal runs on the copy (same options, on the caller's stream
+// or the graph's), from the mapped sources, and a gather puts its values into
+// this graph's result buffer in original IDs. Levels and distances do not
+// depend on the numbering, so the result is the one the original CSR gives;
+// CC labels are mapped to each component's smallest original ID. The
+// report's seconds cover the traversal and the mapping.
 static int run_on_twin(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc, const i2_opts* opts,
                        i2_report* rep) {
   std::vector<int> mapped;
@@ -1078,8 +1106,15 @@ static int run_on_twin(i2_graph* g, int algo, int src, const int* srcs_host, int
   g->last_on_twin = true;
   g->last_iters = g->twin->last_iters;
   const int n = g->g.nodes;
-  k_unpermute<<<(int)std::min<long long>(4LL * sm_count(), (n + 255) / 256), 256, 0, s>>>(g->twin->dist, g->d_inv, n,
-                                                                                          g->dist);
+  const int grid = (int)std::min<long long>(4LL * sm_count(), (n + 255) / 256);
+  if (algo == I2_CC) {
+    int* mn = g->wl[0];  // free while the original CSR is not traversed
+    k_cc_min_init<<<grid, 256, 0, s>>>(mn, n);
+    k_cc_min_original<<<grid, 256, 0, s>>>(g->twin->dist, g->d_inv, n, mn);
+    k_cc_labels<<<grid, 256, 0, s>>>(g->twin->dist, g->d_inv, mn, n, g->dist);
+  } else {
+    k_unpermute<<<grid, 256, 0, s>>>(g->twin->dist, g->d_inv, n, g->dist);
+  }
   I2_CK(cudaGetLastError());
   if (rep) {
     I2_CK(cudaEventRecord(g->ev3, s));
@@ -1097,6 +1132,14 @@ int run_traversal(i2_graph* g, int algo, int src, const int* srcs_host, int nsrc
   if (algo < I2_BFS || algo > I2_MIS) return I2_ERR_ARG;
   I2_CK(cudaSetDevice(g->device));
   if (g->twin && (algo == I2_BFS || algo == I2_SSSP)) return run_on_twin(g, algo, src, srcs_host, nsrc, opts, rep);
+  if (g->twin && algo == I2_CC) {
+    // A component's smallest original ID follows from the copy's labels only
+    // where components are the same vertex sets in both (symmetric edges);
+    // the copy's adjacency is sorted, so its check decides set symmetry.
+    int st = ensure_symmetry(g->twin);
+    if (st) return st;
+    if (g->twin->gs.symmetric == 1) return run_on_twin(g, algo, 0, nullptr, 0, opts, rep);
+  }
   g->last_on_twin = false;
   i2_opts o{};
   if (opts) o = *opts;

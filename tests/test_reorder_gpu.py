@@ -2,8 +2,9 @@
 
 BFS and SSSP run on a copy renumbered by descending degree and their values
 are gathered back to the original IDs; these tests check that every style,
-selector, ordering and loop mode still returns exactly the oracle's levels and
-distances in the original numbering, that CC and MIS are untouched, and that
+selector, ordering and loop mode still returns exactly the oracle's levels,
+distances and minimum-ID labels in the original numbering, that MIS and CC of
+directed graphs keep the original CSR, and that
 dropping, re-tuning and re-weighting a reordered graph keep it right."""
 import numpy as np
 import pytest
@@ -65,9 +66,14 @@ def test_reordered_bfs_sssp_match_oracle_every_style_and_loop(gpu):
                 np.testing.assert_array_equal(d, want_s, err_msg=f"{name} sssp budget {budget} {s}")
             d, _ = dg.sssp(s, variant="vp_cta", delta=256)
             np.testing.assert_array_equal(d, want_s, err_msg=f"{name} sssp delta {s}")
-        # CC and MIS keep the original CSR (their values are IDs)
-        lab, _ = dg.cc(variant="heuristic")
-        np.testing.assert_array_equal(lab, oracle.cc(g), err_msg=f"{name} cc")
+        # CC runs on the copy (symmetric graphs), labels mapped back to each
+        # component's smallest original ID; MIS keeps the original CSR
+        want_c = oracle.cc(g)
+        for v in STYLES + ["union_find"]:
+            for loop in (i2.I2_LOOP_GRAPH, i2.I2_LOOP_HOST):
+                lab, _ = dg.cc(variant=v, loop=loop)
+                np.testing.assert_array_equal(lab, want_c, err_msg=f"{name} cc {v} {loop}")
+        np.testing.assert_array_equal(dg.mis()[0], oracle.mis(g), err_msg=f"{name} mis")
         dg.free()
 
 
@@ -85,9 +91,11 @@ def test_reordered_directed_graph_and_device_results(gpu):
                 dg.run_device(algo, s, out_ptr=out.data_ptr(), variant=v, stream=stream.cuda_stream, report=False)
                 stream.synchronize()
                 np.testing.assert_array_equal(out.cpu().numpy(), ref, err_msg=f"algo {algo} {v} src {s}")
-    # pull styles still refuse a directed graph
+    # pull styles still refuse a directed graph; CC keeps the original CSR
     with pytest.raises(i2.I2Error):
         dg.bfs(0, variant="pull_frontier")
+    for v in ("vp_cta", "heuristic"):
+        np.testing.assert_array_equal(dg.cc(variant=v)[0], oracle.cc(g), err_msg=f"directed cc {v}")
     dg.free()
 
 
