@@ -703,8 +703,8 @@ def run_rmat26(args, rank: int, world: int, local: int):
     """Config: RMAT scale 26 (--scale), 64 seeded sources (--sources; degree
     >= 1) for BFS and SSSP, CC once; the edge-balanced fixed style (SSSP also
     with the budgeted near/far ordering), the heuristic and the learned
-    selector; BFS and SSSP on the graph's degree-ordered copy unless --order
-    none. Sources shard across ranks."""
+    selector; BFS, SSSP and CC on the graph's degree-ordered copy unless
+    --order none. Sources shard across ranks."""
     import torch
 
     import indigo2suite_b200 as i2
@@ -720,7 +720,7 @@ def run_rmat26(args, rank: int, world: int, local: int):
     nsrc = args.sources
     dg = i2.DeviceGraph.generate_rmat(args.scale, 16, 0.57, 0.19, 0.19, seed=args.scale)
     gen_s = time.time() - t0
-    # BFS and SSSP on the degree-ordered copy (CC keeps the original CSR)
+    # BFS, SSSP and CC on the degree-ordered copy, results in original IDs
     t1 = time.time()
     dg.reorder(args.order)
     torch.cuda.synchronize()
@@ -836,7 +836,7 @@ def main():
     ap.add_argument("--rows", default="all",
                     help="rmat26 workload: rows to run (vp_cta, vp_cta_budget, heuristic, learned) or all")
     ap.add_argument("--order", choices=["none", "degree"], default="degree",
-                    help="rmat26 workload: vertex numbering BFS and SSSP run under (degree: a copy "
+                    help="rmat26 workload: vertex numbering BFS, SSSP and CC run under (degree: a copy "
                          "renumbered by descending degree, results in original IDs)")
     ap.add_argument("--loop", choices=["graph", "host", "relaunch"], default="graph",
                     help="graph: one CUDA graph whose resident kernel runs every iteration (default); "
