@@ -111,7 +111,8 @@ typedef struct {
                        (from distance histograms of the frontier, and of the far
                        pile when the frontier runs dry); the rest wait on the far
                        pile. 0: off; > 0: this many edges;
-                       I2_SSSP_BUDGET_AUTO: the engine's default (28672 per SM).
+                       I2_SSSP_BUDGET_AUTO: the engine's default (28672 per SM,
+                       twice that on graphs of 2^30 CSR entries or more).
                        The distances do not depend on it. */
 } i2_opts;
 
@@ -246,8 +247,9 @@ int i2_graph_tune(i2_graph* g, int heavy_threshold, int blocks_per_sm, int smem_
    name side by side, so their values stay in L2 on graphs whose value arrays
    do not fit there (RMAT scale 26: SSSP 1.5x, BFS 1.4-1.9x, CC 1.7x faster).
    Costs a second CSR in device memory (and, while building, scratch of
-   24 bytes per CSR entry) and g.nodes ints on the host. I2_ORDER_NONE drops
-   the copy. Waits for the graph's work and the device. */
+   24 bytes per CSR entry) and g.nodes ints on the host; a graph without
+   edges keeps no copy. I2_ORDER_NONE drops the copy. Waits for the graph's
+   work and the device. */
 enum { I2_ORDER_NONE = 0, I2_ORDER_DEGREE = 1 };
 int i2_graph_reorder(i2_graph* g, int order);
 /* Give the graph the reference's synthetic weights when it has none (on the device). */

@@ -107,6 +107,7 @@ static int csr_from_keys(unsigned long long* k0, unsigned long long* k1, int* w0
   void* tmp = nullptr;
   size_t tb = 0, tb2 = 0;
   cudaError_t e = sc.get(&d_num, sizeof(long long));
+  if (e == cudaSuccess) e = cudaMemset(d_num, 0, sizeof(long long));  // stays 0 for an empty key set
   if (e != cudaSuccess) return cuda_status(e);
   const bool given = cw.mode == 2;
   cub::DoubleBuffer<unsigned long long> dk(k0, k1);

@@ -133,3 +133,20 @@ def test_reorder_rejects_unknown_order(gpu):
     dg = i2.DeviceGraph.upload(i2.gen_rmat(10, 8, seed=66))
     assert i2.lib.i2_graph_reorder(dg._h, 7) == i2.capi.I2_ERR_ARG
     dg.free()
+
+
+def test_reorder_tiny_and_edgeless_graphs(gpu):
+    graphs = {
+        "edgeless": i2.ECLGraph(5, 0, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)),
+        "one_vertex": i2.ECLGraph(1, 0, np.zeros(2, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)),
+        "one_edge": i2.ECLGraph(3, 2, np.array([0, 1, 1, 2], np.int32), np.array([2, 0], np.int32),
+                                np.array([7, 7], np.int32)),
+    }
+    for name, g in graphs.items():
+        dg = i2.DeviceGraph.upload(g)
+        dg.reorder("degree")
+        for s in range(g.nodes):
+            np.testing.assert_array_equal(dg.bfs(s)[0], oracle.bfs(g, s), err_msg=f"{name} bfs {s}")
+            np.testing.assert_array_equal(dg.sssp(s)[0], oracle.sssp(g, s), err_msg=f"{name} sssp {s}")
+        np.testing.assert_array_equal(dg.cc(variant="heuristic")[0], oracle.cc(g), err_msg=f"{name} cc")
+        dg.free()
